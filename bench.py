@@ -1,0 +1,333 @@
+"""Benchmark of the ELP ring-melt sweep: attempted monomer moves per second.
+
+One bench step is one Monte Carlo time step (N*P attempted monomer moves, the
+reference efpol's unit, cpupol/efpol_lib.c:123) of the workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl elp|reference]
+
+Default workload: the single large ring melt L=128, N=1000, density 1.2
+(2517 rings), seed 7, initialised like the reference's CreatePolymers
+(synthetic: no dataset exists for this path).  The lattice (8 MB) is smaller
+than L2, so L2 is flushed between timed steps (a 256 MB write outside the
+timed events).  Extra legs on rank 0: the L=256, N=5000 melt (roofline
+configuration), the reference CPU efpol timed on this host, and the
+end-to-end path through the C ABI with host buffers.
+
+--gpus N runs N independent replicas (one process per GPU, seeds offset by
+rank); there is no data-path collective -- replicas only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "mc-polymer-simulation_b200", "python"))
+
+METRIC = "attempted monomer moves/s"
+UNIT = "moves/s"
+WORKLOADS = {
+    "L128": dict(L=128, N=1000, seed=7, density=1.2),
+    "L256": dict(L=256, N=5000, seed=11, density=1.2),
+    "L32": dict(L=32, N=100, seed=1, density=1.2),
+}
+
+
+def npol(w):
+    return max(1, int(w["density"] * w["L"] ** 3 / w["N"] + 0.5))
+
+
+def algo_bytes(w):
+    """Algorithmic bytes of one sweep: every uint32 site word read and written
+    once, every int8 bond read and written once: 8*S + 2*M."""
+    return 8 * w["L"] ** 3 + 2 * w["N"] * npol(w)
+
+
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(name)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(w, steps, threads=1):
+    """Reference efpol (built from the reference sources into oracle/_ref) timed
+    on this host: `threads` independent processes, each `steps` MC steps."""
+    ref = os.path.join(REPO, "oracle", "_ref", "ref_bench")
+    kind = "reference"
+    if not os.path.exists(ref):
+        ref = os.path.join(REPO, "oracle", "efpol_port")
+        kind = "port"
+        if not os.path.exists(ref):
+            subprocess.run(["make", "-C", os.path.join(REPO, "oracle")], check=True, stdout=subprocess.DEVNULL)
+    t0 = time.perf_counter()
+    procs = [subprocess.Popen([ref, str(w["L"]), str(w["N"]), str(w["density"]), str(w["seed"] + i), str(steps)],
+                              stdout=subprocess.PIPE, text=True) for i in range(threads)]
+    outs = [json.loads(p.communicate()[0].strip().splitlines()[-1]) for p in procs]
+    wall = time.perf_counter() - t0
+    moves = sum(o["moves"] for o in outs)
+    # processes run concurrently; each times its own DoMCStep window
+    rate = moves / max(o["seconds"] for o in outs)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{steps} MC steps of L={w['L']} N={w['N']} per process, {threads} process(es), "
+                      f"{moves:.3g} attempted moves in {wall:.2f} s"}
+
+
+def run_elp(args, rank, world):
+    import torch
+    import elp
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    w = WORKLOADS[args.workload]
+    M = w["N"] * npol(w)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+
+    m = elp.Melt(L=w["L"], N=w["N"], seed=w["seed"] + rank, device=dev)
+    m.init_melt()
+    m.run(args.warmup)
+    m.sync()
+    info = m.info()
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    times = []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            times.append(m.run_timed(1))
+    torch.cuda.synchronize()
+    total_ms = sum(times)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps * M / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+    assert m.check() == 0, "integrity check failed after the timed run"
+
+    peak, peak_kind = measured_peak()
+    achieved = algo_bytes(w) / (ms_per_step / 1e3) / 1e9
+    tr = profile_traffic(args.workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference CreatePolymers initial melt)",
+        "config": {"workload": f"ring melt L={w['L']} N={w['N']} density={w['density']} P={npol(w)} "
+                               f"seed={w['seed']}, one sweep kernel per step",
+                   "L": w["L"], "N": w["N"], "P": npol(w), "sites": w["L"] ** 3, "monomers": M,
+                   "geometry": {"periodic": info.periodic, "tile": list(info.tile), "ncol": info.ncol,
+                                "domains": info.domains, "threads": info.threads},
+                   "l2": "flushed between timed steps (256 MB write outside the timed events)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_bytes(w),
+                     "traffic": tr},
+        "gpu_launches": args.steps,
+    }
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+
+    if rank == 0 and not args.no_extras:
+        line["e2e"] = e2e_leg(elp, w, dev, args)
+        line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps)
+        if args.workload != "L256" and not args.no_l256:
+            line["L256"] = l256_leg(elp, torch, dev, flush, args)
+    return line
+
+
+def e2e_leg(elp, w, dev, args):
+    """Through the C ABI with host buffers: per bench step, load the rings from
+    pinned host memory (H2D), run one dump interval, fetch them back (D2H)."""
+    import numpy as np
+    import torch
+
+    interval = args.e2e_interval
+    P, N = npol(w), w["N"]
+    m = elp.Melt(L=w["L"], N=N, seed=w["seed"], device=dev)
+    m.init_melt()
+    m.run(args.warmup)
+    start_t = torch.empty((P, 3), dtype=torch.int32).pin_memory()
+    bonds_t = torch.empty((P, N), dtype=torch.uint8).pin_memory()
+    start, bonds = start_t.numpy(), bonds_t.numpy()
+    s0, b0 = m.fetch()
+    start[:], bonds[:] = s0, b0
+    reps = max(2, args.e2e_reps)
+    t0 = time.perf_counter()
+    step = m.step
+    for _ in range(reps):
+        m.load_chains(start, bonds, step)
+        m.run(interval)
+        s1, b1 = m.fetch()
+        start[:], bonds[:] = s1, b1
+        step += interval
+    dt = time.perf_counter() - t0
+    assert m.check() == 0
+    S = w["L"] ** 3
+    return {"value": reps * interval * N * P / dt, "unit": UNIT,
+            "h2d_bytes_per_step": 4 * S + 16 * P, "d2h_bytes_per_step": 12 * P + N * P,
+            "steps_per_call": interval,
+            "path": "elp_load_chains(host) + elp_run(interval) + elp_fetch_chains(host), wall clock"}
+
+
+def l256_leg(elp, torch, dev, flush, args):
+    w = WORKLOADS["L256"]
+    M = w["N"] * npol(w)
+    m = elp.Melt(L=w["L"], N=w["N"], seed=w["seed"], device=dev)
+    m.init_melt()
+    m.run(3)
+    m.sync()
+    times = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        times.append(m.run_timed(1))
+    ms = sum(times) / len(times)
+    peak, _ = measured_peak()
+    achieved = algo_bytes(w) / (ms / 1e3) / 1e9
+    return {"workload": "ring melt L=256 N=5000 P=4027 seed=11", "value": M / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_launch": algo_bytes(w), "traffic": profile_traffic("L256")}}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    w = WORKLOADS[args.workload]
+    threads = os.cpu_count() or 1
+    steps_per = max(1, args.ref_steps)
+    tot_moves, tot_wall = 0.0, 0.0
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(w, steps_per, threads)
+        if i >= args.warmup:
+            moves = threads * steps_per * w["N"] * npol(w)
+            tot_moves += moves
+            tot_wall += moves / cb["value"]
+    value = tot_moves / tot_wall
+    cb["value"] = value
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_wall / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (reference CreatePolymers initial melt)",
+            "config": {"workload": f"ring melt L={w['L']} N={w['N']} density={w['density']} P={npol(w)}; each step "
+                                   f"= {steps_per} MC steps per process on {threads} host cores",
+                       "L": w["L"], "N": w["N"], "P": npol(w)},
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="elp", choices=["elp", "reference"])
+    ap.add_argument("--workload", default="L128", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--ref-steps", type=int, default=8)
+    ap.add_argument("--e2e-interval", type=int, default=100)
+    ap.add_argument("--e2e-reps", type=int, default=5)
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-l256", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_reference(args, rank, world) if args.impl == "reference" else run_elp(args, rank, world)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,139 @@
+/*
+ * elp.h -- C ABI of the B200 Elastic Lattice Polymer (ELP) sweep engine.
+ *
+ * Plain C types only: a caller binds this from C (the drop-in front-ends),
+ * ctypes, cgo or JNI without any C++ or torch types.
+ *
+ * Mapping onto the reference:
+ *   elp_create + elp_init_melt   <- SimPropDefaultInit/LoadPolymers/GPULibInit/
+ *                                   GPULibLoadBuffers (gpupol2/gpupol_cuda.h:6-7,
+ *                                   gpupol2/gpupol_init.c:83-152) and efpol's
+ *                                   CSInit/SetTransTable/CreatePolymers
+ *                                   (cpupol/efpol.c:60-66, cpupol/efpol_init.c:239-424)
+ *   elp_run                      <- GPULibRun(nTime) (gpupol2/gpupol_cuda.h:9) and
+ *                                   DoMCStep(nTime) (cpupol/efpol_lib.c:122)
+ *   elp_fetch_chains             <- GPULatticeToCPU (gpupol2/gpupol_cuda.h:11)
+ *   elp_write_tuv / elp_load_tuv <- WriteLatticeFile / ReadLatticeFile
+ *                                   (cpupol/efpol_io.c:3-77, gpupol2/gpupol_io.c:105-203)
+ *   elp_check                    <- CheckIntegrity (cpupol/efpol_io.c:158-211)
+ *   elp_destroy                  <- GPULibRelease (gpupol2/gpupol_cuda.h:8)
+ *
+ * Errors: every call returns an elp_status; nothing calls exit() or aborts.
+ * elp_last_error() gives a message for the calling thread's last failure.
+ * Threading: one host thread per context at a time.
+ */
+#ifndef ELP_H
+#define ELP_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t elp_status;
+#define ELP_OK 0
+#define ELP_ERR_ARG 1         /* invalid argument or geometry */
+#define ELP_ERR_CUDA 2        /* CUDA error or no CUDA device */
+#define ELP_ERR_NOMEM 3       /* device or host allocation failed */
+#define ELP_ERR_IO 4          /* file could not be opened / written */
+#define ELP_ERR_FORMAT 5      /* TUV text malformed or does not match the job */
+#define ELP_ERR_INTEGRITY 6   /* configuration violates an ELP invariant */
+#define ELP_ERR_STATE 7       /* call not valid in the context's state */
+#define ELP_ERR_BUSY 8        /* server/queue full or admission refused */
+
+typedef struct elp_ctx elp_ctx;
+
+typedef struct elp_job_spec {
+    int32_t L;                /* cubic box edge (sites) */
+    int32_t N;                /* monomers per ring */
+    int32_t P;                /* rings; <= 0: round(density * L^3 / N) as GetNPol */
+    double density;           /* monomers per site, used when P <= 0 */
+    uint32_t seed;            /* Philox key word 0 */
+    uint32_t salt;            /* Philox key word 1 (independent streams) */
+    int32_t periodic;         /* -1 auto, 0 tiled domains, 1 whole box on chip */
+    int32_t tile[3];          /* tiled domain edges, 0 = auto */
+    int32_t ncol;             /* colour modulus, 0 = auto */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t steps_per_launch; /* whole-box domains: steps per kernel launch (>=1) */
+} elp_job_spec;
+
+typedef struct elp_info {
+    int32_t L, N, P;
+    int32_t periodic, tile[3], ncol;
+    int32_t domains;          /* CTAs per step */
+    int32_t threads;          /* threads per CTA */
+    uint64_t smem_bytes;      /* dynamic shared memory per CTA */
+    uint64_t step;            /* absolute steps done */
+    uint64_t device_bytes;    /* device memory held by the context */
+} elp_info;
+
+/* Fill a spec with defaults: density 1.2, auto geometry, device 0. */
+void elp_default_spec(elp_job_spec* spec);
+
+/* Create a context: validates the geometry, allocates device state, uploads
+ * the transition table.  The lattice starts empty (use elp_init_melt or a
+ * load call). */
+elp_status elp_create(const elp_job_spec* spec, elp_ctx** out);
+
+/* Reference initial melt (CreatePolymers): step counter reset to 0. */
+elp_status elp_init_melt(elp_ctx* ctx);
+
+/* Load rings from chain form: start[3*P] = (t,u,v) of monomer 0 in [0,L),
+ * bonds[P*N] = 4-bit bond codes (TUV order).  `step` sets the absolute step
+ * counter, so a run resumed from a dump continues the same random stream. */
+elp_status elp_load_chains(elp_ctx* ctx, const int32_t* start, const uint8_t* bonds, uint64_t step);
+
+/* Load a TUV file (LT/LU/LV/np/maxPolLength header, len= blocks). */
+elp_status elp_load_tuv(elp_ctx* ctx, const char* path, uint64_t step);
+
+/* Run n time steps (1 step = N*P attempted monomer moves).  Asynchronous:
+ * stream-ordered on the context's stream; returns after enqueueing. */
+elp_status elp_run(elp_ctx* ctx, int64_t nsteps);
+
+/* Same as elp_run, timed with CUDA events recorded on the context's stream
+ * around the launches; blocks and returns the elapsed milliseconds. */
+elp_status elp_run_timed(elp_ctx* ctx, int64_t nsteps, float* ms);
+
+elp_status elp_sync(elp_ctx* ctx);
+
+/* Rebuild the rings on the device and copy them to host buffers
+ * start[3*P] (int32) and bonds[P*N] (uint8).  Blocking.  Returns
+ * ELP_ERR_INTEGRITY if a ring cannot be walked. */
+elp_status elp_fetch_chains(elp_ctx* ctx, int32_t* start, uint8_t* bonds);
+
+/* Write the current state as a TUV file, byte-compatible with the
+ * reference's WriteLatticeFile.  Blocking. */
+elp_status elp_write_tuv(elp_ctx* ctx, const char* path);
+
+/* Integrity check on the device.  *code: 0 ok, 3 two rings share a site,
+ * 4 invalid bond, broken ring, bad count or bookkeeping (efpol's codes). */
+elp_status elp_check(elp_ctx* ctx, int32_t* code);
+
+elp_status elp_get_info(const elp_ctx* ctx, elp_info* info);
+
+/* Raw state: words[L^3] site words, records[4*P]. Blocking. */
+elp_status elp_get_state(elp_ctx* ctx, uint32_t* words, uint32_t* records);
+elp_status elp_set_state(elp_ctx* ctx, const uint32_t* words, const uint32_t* records, uint64_t step);
+
+/* Moves accepted since creation (counted on the device). */
+elp_status elp_accepted(elp_ctx* ctx, uint64_t* accepted);
+
+void elp_destroy(elp_ctx* ctx);
+
+/* The 4096-entry transition table (dst1 | dst2<<4 per option), identical to
+ * the reference's transTable & 0xff for sl_equal (cpupol/efpol_init.c:314). */
+elp_status elp_transition_table(uint8_t out[4096]);
+
+/* Format chains as TUV text.  *len receives the length (excluding NUL);
+ * with buf == NULL only the length is computed. */
+elp_status elp_format_tuv(int32_t L, int32_t N, int32_t P, const int32_t* start, const uint8_t* bonds,
+                          char* buf, size_t cap, size_t* len);
+
+const char* elp_status_string(elp_status s);
+const char* elp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

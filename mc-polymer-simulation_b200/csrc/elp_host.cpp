@@ -1,0 +1,278 @@
+// elp_host.cpp -- host-side core of the ELP engine: geometry policy,
+// shared-memory layout, the transition table, the initial melt and the
+// conversion between chain form (start site + bond string, the TUV content)
+// and site words.
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "elp_internal.h"
+
+// ---- colouring -------------------------------------------------------------
+// Same-colour sites (x + 2y + 3z = c mod n) must be at least three bonds
+// apart so that two anchors' radius-1 footprints never meet: no sum of two
+// bonds (other than 0) may have colour 0.
+static int colour_ok(int n)
+{
+    if (n < 13) return 0;
+    for (uint32_t a = 0; a < 16; a++) {
+        if (a && !elp_valid_bond(a)) continue;
+        for (uint32_t b = 0; b < 16; b++) {
+            if (b && !elp_valid_bond(b)) continue;
+            int dt = elp_bt(a) + elp_bt(b), du = elp_bu(a) + elp_bu(b), dv = elp_bv(a) + elp_bv(b);
+            if (!dt && !du && !dv) continue;
+            int c = ((dt + 2 * du + 3 * dv) % n + n) % n;
+            if (c == 0) return 0;
+        }
+    }
+    return 1;
+}
+
+// Smallest valid colour modulus that divides m (16 preferred).
+int elp_pick_ncol(int m)
+{
+    if (m % 16 == 0) return 16;
+    for (int n = 13; n <= m; n++)
+        if (m % n == 0 && colour_ok(n)) return n;
+    return 0;
+}
+
+int elp_geometry_ok(const elp_geometry* g)
+{
+    if (!g || g->L < 5 || g->L > 1024) return 0;
+    if (!colour_ok(g->ncol)) return 0;
+    if (g->periodic) {
+        if (g->tx != g->L || g->ty != g->L || g->tz != g->L) return 0;
+        if (g->L % g->ncol) return 0;
+    } else {
+        if (g->tx < 3 || g->ty < 3 || g->tz < 3) return 0;
+        if (g->L % g->tx || g->L % g->ty || g->L % g->tz) return 0;
+        if (g->tx % g->ncol) return 0;
+    }
+    long R = (long)g->ty * g->tz;
+    long A = R * (g->tx / g->ncol);
+    if (A % 4) return 0;
+    if (A / 4 > 1024) return 0;
+    elp_smem_layout lay;
+    elp_layout(g, &lay);
+    if (lay.bytes > 227u * 1024u) return 0;
+    return 1;
+}
+
+// Worst shared-memory bank multiplicity of the first anchor load of a warp,
+// over all colours and warps.
+static int bank_cost(const elp_geometry* g, int ox, int sx, int sxy)
+{
+    int n = g->ncol, ty = g->ty, tz = g->tz;
+    long R = (long)ty * tz, A = R * (g->tx / n), G = A / 4;
+    int worst = 1;
+    for (int c = 0; c < n; c++) {
+        for (long w0 = 0; w0 < G && w0 < 32 * 8; w0 += 32) {
+            int cnt[32] = {0};
+            for (long g0 = w0; g0 < w0 + 32 && g0 < G; g0++) {
+                long j = g0 / R, row = g0 % R;
+                int y = (int)(row % ty), z = (int)(row / ty);
+                int x = (((c - 2 * y - 3 * z) % n) + n) % n + n * (int)j;
+                long idx = ox + x + (long)sx * y + (long)sxy * z;
+                int b = (int)(idx & 31);
+                if (++cnt[b] > worst) worst = cnt[b];
+            }
+        }
+    }
+    return worst;
+}
+
+void elp_layout(const elp_geometry* g, elp_smem_layout* lay)
+{
+    int halo = g->periodic ? 0 : 2;
+    int best_sx = 0, best_sxy = 0, best = 1 << 30;
+    for (int px = 0; px < 8; px++) {
+        int sx = g->tx + halo + px;
+        for (int pz = 0; pz < 32; pz += 1) {
+            int sxy = sx * (g->ty + halo) + pz;
+            int ox = g->periodic ? 0 : 1 + sx + sxy;
+            int cost = bank_cost(g, ox, sx, sxy) * 64 + px + pz;  // prefer small padding
+            if (cost < best) { best = cost; best_sx = sx; best_sxy = sxy; }
+        }
+    }
+    lay->sx = best_sx;
+    lay->sxy = best_sxy;
+    lay->ox = g->periodic ? 0 : 1 + best_sx + best_sxy;
+    lay->words = best_sxy * (g->tz + halo);
+    lay->anchors = g->ty * g->tz * (g->tx / g->ncol);
+    lay->groups = lay->anchors / 4;
+    lay->bytes = (size_t)lay->words * 4 + 4096 + 27 * 16 * 4 + 64 * 4;
+}
+
+// ---- Philox4x32-10 (host copy; Salmon et al. SC'11) --------------------------
+void elp_philox_host(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c1 = (uint32_t)p1; c3 = (uint32_t)p0; c0 = n0; c2 = n2;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// ---- transition table (sl_equal, rings): cpupol/efpol_init.c:285-424 --------
+// Built by the same steps as the reference so that the 16 options of every
+// (b_{m-1}, b_m) row, with their multiplicities and order, are identical.
+namespace {
+struct TableBuilder {
+    uint32_t e[4096];
+    int cnt[256];
+    void add(uint32_t s1, uint32_t s2, uint32_t d1, uint32_t d2)
+    {
+        int id = 256 * (int)s1 + 16 * (int)s2 + cnt[16 * s1 + s2];
+        if (id < 4096) e[id] = d1 | (d2 << 4);
+        cnt[16 * s1 + s2]++;
+    }
+};
+int sum_bond(uint32_t a, uint32_t b, uint32_t* c)
+{
+    if ((a | b) != 0xf && (a & b)) return 0;
+    *c = ((a | b) == 0xf) ? (a & b) : (a | b);
+    return elp_valid_bond(*c);
+}
+}  // namespace
+
+void elp_build_table(uint8_t tab[4096])
+{
+    TableBuilder T;
+    memset(&T, 0, sizeof(T));
+    for (uint32_t a = 1; a < 0xf; a++) {
+        if (!elp_valid_bond(a)) continue;
+        for (uint32_t b = a + 1; b < 0xf; b++) {
+            uint32_t r;
+            if (!elp_valid_bond(b) || !sum_bond(a, b, &r)) continue;
+            T.add(a, b, r, 0); T.add(a, b, 0, r); T.add(b, a, r, 0); T.add(b, a, 0, r);
+            T.add(r, 0, a, b); T.add(r, 0, b, a); T.add(0, r, a, b); T.add(0, r, b, a);
+        }
+    }
+    for (uint32_t b = 1; b < 0xf; b++) {
+        if (!elp_valid_bond(b)) continue;
+        for (int i = 0; i < 4; i++) { T.add(0, b, b, 0); T.add(b, 0, 0, b); }
+    }
+    for (uint32_t u1 = 1; u1 < 0xf; u1++) {
+        if (!elp_valid_bond(u1)) continue;
+        for (uint32_t u2 = 1; u2 < 0xf; u2++) {
+            uint32_t r;
+            if (!elp_valid_bond(u2) || !sum_bond(u1, (~u2) & 0xf, &r)) continue;
+            for (uint32_t u3 = 1; u3 < 0xf; u3++) {
+                if (!elp_valid_bond(u3)) continue;
+                int kink = sum_bond(u1, u3, &r);
+                for (uint32_t u4 = 1; u4 < 0xf; u4++) {
+                    if (!elp_valid_bond(u4)) continue;
+                    if (elp_bt(u1) + elp_bt(u3) != elp_bt(u2) + elp_bt(u4)) continue;
+                    if (elp_bu(u1) + elp_bu(u3) != elp_bu(u2) + elp_bu(u4)) continue;
+                    if (elp_bv(u1) + elp_bv(u3) != elp_bv(u2) + elp_bv(u4)) continue;
+                    int copies = kink ? 6 : 2;
+                    for (int i = 0; i < copies; i++) T.add(u1, u3, u2, u4);
+                }
+            }
+        }
+    }
+    for (int row = 0; row < 256; row++)
+        for (int want = 2; want <= 8; want *= 2)
+            if (T.cnt[row] == want)
+                for (int i = 0; i < want; i++) {
+                    uint32_t v = T.e[row * 16 + i];
+                    T.add((uint32_t)row / 16, (uint32_t)row % 16, v & 0xf, (v >> 4) & 0xf);
+                }
+    for (uint32_t a = 0; a < 0xf; a++) {
+        if (!elp_valid_bond(a)) continue;
+        T.add(a, 0xf, 0x0, 0xf); T.add(0xf, a, 0xf, 0x0);  // linear-chain ends (sl_equal: once)
+        T.add(0x0, 0xf, a, 0xf); T.add(0xf, 0x0, 0xf, a);
+    }
+    for (int row = 0; row < 256; row++)
+        while (T.cnt[row] < 16) T.add((uint32_t)row / 16, (uint32_t)row % 16, 0, 0);
+    for (int i = 0; i < 4096; i++) tab[i] = (uint8_t)(T.e[i] & 0xff);
+}
+
+// GetNPol, cpupol/efpol_lib.c:50-56
+int elp_get_npol(double density, int N, long sites)
+{
+    return (int)(density * (double)sites / (double)N + 0.5);
+}
+
+// CreatePolymers, cpupol/efpol_init.c:239-283: rings on a delta-spaced grid,
+// monomer 0 alone, bond +v, the other N-1 monomers stored on the next site,
+// closing bond -v.  Returns 0, or 1 if the grid cannot hold P rings.
+int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds)
+{
+    if (N < 3 || P < 1) return 1;
+    int delta;
+    for (delta = 1; delta < L; delta++) {
+        long ntot = (long)(L / delta) * (L / delta) * (L / (delta + 1));
+        if (ntot < P) { delta--; break; }
+    }
+    if (delta < 1 || delta >= L) return 1;
+    int nt = L / delta, nv = L / (delta + 1);
+    if ((long)nt * nv * (L / delta) < P) return 1;
+    for (int p = 0; p < P; p++) {
+        start[3 * p] = delta * (p % nt);
+        start[3 * p + 1] = delta * (p / nt / nv);
+        start[3 * p + 2] = (delta + 1) * ((p / nt) % nv);
+        uint8_t* b = bonds + (size_t)p * N;
+        memset(b, 0, (size_t)N);
+        b[0] = 0x4;
+        b[N - 1] = 0xb;
+    }
+    return 0;
+}
+
+static inline uint32_t wrap_site(int L, long t, long u, long v)
+{
+    t %= L; u %= L; v %= L;
+    if (t < 0) t += L;
+    if (u < 0) u += L;
+    if (v < 0) v += L;
+    return (uint32_t)(t + (long)L * (u + (long)L * v));
+}
+
+int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t* bonds, uint32_t* lat, uint32_t* rec)
+{
+    size_t S = (size_t)L * L * L;
+    memset(lat, 0, S * sizeof(uint32_t));
+    std::vector<uint32_t> pos((size_t)N);
+    for (int p = 0; p < P; p++) {
+        const uint8_t* b = bonds + (size_t)p * N;
+        long t = start[3 * p], u = start[3 * p + 1], v = start[3 * p + 2];
+        if (t < 0 || u < 0 || v < 0 || t >= L || u >= L || v >= L) return 4;
+        int nz = 0;
+        for (int m = 0; m < N; m++) {
+            pos[(size_t)m] = wrap_site(L, t, u, v);
+            if (b[m] && !elp_valid_bond(b[m])) return 4;
+            t += elp_bt(b[m]); u += elp_bu(b[m]); v += elp_bv(b[m]);
+            nz += b[m] ? 1 : 0;
+        }
+        if (wrap_site(L, t, u, v) != pos[0] || nz < 2) return 4;
+        int first = 0;
+        while (!b[(first + N - 1) % N]) first++;
+        int m = first, done = 0;
+        while (done < N) {
+            int len = 1;
+            while (b[(m + len - 1) % N] == 0) len++;
+            uint32_t site = pos[(size_t)m];
+            if (lat[site]) return 3;
+            uint32_t bo = b[(m + len - 1) % N];
+            int off0 = (N - m) % N;
+            if (off0 < len) {
+                lat[site] = bo | ELP_LBIT | ((uint32_t)p << 5);
+                rec[ELP_REC_WORDS * p + 0] = site;
+                rec[ELP_REC_WORDS * p + 1] = (uint32_t)len;
+                rec[ELP_REC_WORDS * p + 2] = (uint32_t)off0;
+                rec[ELP_REC_WORDS * p + 3] = 0;
+            } else {
+                lat[site] = bo | ((uint32_t)len << 5);
+            }
+            done += len;
+            m = (m + len) % N;
+        }
+    }
+    return 0;
+}

@@ -1,0 +1,206 @@
+"""ctypes binding of lib/libelp.so (the C ABI declared in include/elp.h).
+
+This is what the tests and bench.py use to drive the engine; it adds no logic
+of its own.  The library must exist (``make -C mc-polymer-simulation_b200``);
+there is no fallback: every call goes to the sm_100a kernels through the
+C ABI, and a missing library or device raises ``ElpError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libelp.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_IO, ERR_FORMAT, ERR_INTEGRITY, ERR_STATE, ERR_BUSY = range(9)
+
+
+class ElpError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"elp status {status}: {msg}")
+        self.status = status
+
+
+class JobSpec(C.Structure):
+    _fields_ = [("L", C.c_int32), ("N", C.c_int32), ("P", C.c_int32), ("density", C.c_double),
+                ("seed", C.c_uint32), ("salt", C.c_uint32), ("periodic", C.c_int32), ("tile", C.c_int32 * 3),
+                ("ncol", C.c_int32), ("device", C.c_int32), ("steps_per_launch", C.c_int32)]
+
+
+class Info(C.Structure):
+    _fields_ = [("L", C.c_int32), ("N", C.c_int32), ("P", C.c_int32), ("periodic", C.c_int32),
+                ("tile", C.c_int32 * 3), ("ncol", C.c_int32), ("domains", C.c_int32), ("threads", C.c_int32),
+                ("smem_bytes", C.c_uint64), ("step", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
+EXPORTED = [
+    "elp_default_spec", "elp_create", "elp_init_melt", "elp_load_chains", "elp_load_tuv", "elp_run",
+    "elp_run_timed", "elp_sync", "elp_fetch_chains", "elp_write_tuv", "elp_check", "elp_get_info",
+    "elp_get_state", "elp_set_state", "elp_accepted", "elp_destroy", "elp_transition_table",
+    "elp_format_tuv", "elp_status_string", "elp_last_error",
+]
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ElpError(ERR_STATE, f"{LIB_PATH} not built (run make -C {PKG})")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, u32, i64, u64 = C.c_void_p, C.c_int32, C.c_uint32, C.c_int64, C.c_uint64
+    sig = {
+        "elp_default_spec": (None, [vp]),
+        "elp_create": (i32, [vp, vp]),
+        "elp_init_melt": (i32, [vp]),
+        "elp_load_chains": (i32, [vp, vp, vp, u64]),
+        "elp_load_tuv": (i32, [vp, C.c_char_p, u64]),
+        "elp_run": (i32, [vp, i64]),
+        "elp_run_timed": (i32, [vp, i64, vp]),
+        "elp_sync": (i32, [vp]),
+        "elp_fetch_chains": (i32, [vp, vp, vp]),
+        "elp_write_tuv": (i32, [vp, C.c_char_p]),
+        "elp_check": (i32, [vp, vp]),
+        "elp_get_info": (i32, [vp, vp]),
+        "elp_get_state": (i32, [vp, vp, vp]),
+        "elp_set_state": (i32, [vp, vp, vp, u64]),
+        "elp_accepted": (i32, [vp, vp]),
+        "elp_destroy": (None, [vp]),
+        "elp_transition_table": (i32, [vp]),
+        "elp_format_tuv": (i32, [i32, i32, i32, vp, vp, vp, C.c_size_t, vp]),
+        "elp_status_string": (C.c_char_p, [i32]),
+        "elp_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != OK:
+        raise ElpError(status, lib().elp_last_error().decode(errors="replace"))
+
+
+def transition_table() -> np.ndarray:
+    out = np.zeros(4096, dtype=np.uint8)
+    check(lib().elp_transition_table(out.ctypes.data))
+    return out
+
+
+def format_tuv(L, start, bonds) -> str:
+    start = np.ascontiguousarray(start, dtype=np.int32)
+    bonds = np.ascontiguousarray(bonds, dtype=np.uint8)
+    P, N = bonds.shape
+    n = C.c_size_t()
+    check(lib().elp_format_tuv(L, N, P, start.ctypes.data, bonds.ctypes.data, None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib().elp_format_tuv(L, N, P, start.ctypes.data, bonds.ctypes.data, buf, n.value + 1, C.byref(n)))
+    return buf.raw[:n.value].decode()
+
+
+def spec(L=32, N=100, P=0, density=1.2, seed=1, salt=0, periodic=-1, tile=(0, 0, 0), ncol=0, device=0,
+         steps_per_launch=1) -> JobSpec:
+    s = JobSpec()
+    lib().elp_default_spec(C.byref(s))
+    s.L, s.N, s.P, s.density, s.seed, s.salt = L, N, P, density, seed, salt
+    s.periodic = periodic
+    s.tile[0], s.tile[1], s.tile[2] = tile
+    s.ncol, s.device, s.steps_per_launch = ncol, device, steps_per_launch
+    return s
+
+
+class Melt:
+    """One ring melt on one GPU (an elp_ctx)."""
+
+    def __init__(self, **kw):
+        self.h = C.c_void_p()
+        check(lib().elp_create(C.byref(spec(**kw)), C.byref(self.h)))
+        i = self.info()
+        self.L, self.N, self.P = i.L, i.N, i.P
+
+    def info(self) -> Info:
+        i = Info()
+        check(lib().elp_get_info(self.h, C.byref(i)))
+        return i
+
+    @property
+    def step(self) -> int:
+        return self.info().step
+
+    def init_melt(self):
+        check(lib().elp_init_melt(self.h))
+
+    def load_chains(self, start, bonds, step=0):
+        start = np.ascontiguousarray(start, dtype=np.int32)
+        bonds = np.ascontiguousarray(bonds, dtype=np.uint8)
+        assert start.shape == (self.P, 3) and bonds.shape == (self.P, self.N)
+        check(lib().elp_load_chains(self.h, start.ctypes.data, bonds.ctypes.data, step))
+
+    def load_tuv(self, path, step=0):
+        check(lib().elp_load_tuv(self.h, path.encode(), step))
+
+    def run(self, nsteps):
+        check(lib().elp_run(self.h, nsteps))
+
+    def run_timed(self, nsteps) -> float:
+        ms = C.c_float()
+        check(lib().elp_run_timed(self.h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        check(lib().elp_sync(self.h))
+
+    def fetch(self):
+        start = np.zeros((self.P, 3), dtype=np.int32)
+        bonds = np.zeros((self.P, self.N), dtype=np.uint8)
+        check(lib().elp_fetch_chains(self.h, start.ctypes.data, bonds.ctypes.data))
+        return start, bonds
+
+    def write_tuv(self, path):
+        check(lib().elp_write_tuv(self.h, path.encode()))
+
+    def check(self) -> int:
+        code = C.c_int32()
+        check(lib().elp_check(self.h, C.byref(code)))
+        return code.value
+
+    def state(self):
+        w = np.zeros(self.L ** 3, dtype=np.uint32)
+        r = np.zeros((self.P, 4), dtype=np.uint32)
+        check(lib().elp_get_state(self.h, w.ctypes.data, r.ctypes.data))
+        return w, r
+
+    def set_state(self, words, records, step):
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        records = np.ascontiguousarray(records, dtype=np.uint32)
+        check(lib().elp_set_state(self.h, words.ctypes.data, records.ctypes.data, step))
+
+    def accepted(self) -> int:
+        v = C.c_uint64()
+        check(lib().elp_accepted(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().elp_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,116 @@
+"""Regenerate the golden fixtures in this directory from the REFERENCE itself.
+
+Run in a checkout where the reference sources are available:
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+It compiles the reference's efpol from its own sources (oracle/Makefile target
+``ref``; outputs only under oracle/_ref/), then records
+
+* ``table_<model>.npz``  -- the reference's LookupTables for sl_equal,
+  sl_double and sl_quad (cpupol/efpol_init.c:314-424), via oracle/ref_table_dump.c;
+* ``efpol_L32_N100_s1_t{0,100,200}.res.gz`` -- the reference's own TUV dumps
+  for the plain ring melt L=32, N=100, density 1.2, seed 1;
+* ``efpol_L16_N50_s3_t{0..100}.res.gz`` -- a short reference trajectory, one
+  dump every 10 steps (pins the oracle's restatement step for step);
+* ``efpol_stats_L16_N50.json`` / ``efpol_stats_L32_N100.json`` -- ensemble
+  statistics of reference efpol runs (several seeds) computed with
+  oracle/observables.py: Rg^2, stored-length fraction, run-length histogram and
+  centre-of-mass MSD, with per-seed values for error bars.
+
+Nothing at test time reads the reference; the tests read these files only.
+"""
+from __future__ import annotations
+
+import argparse
+import gzip
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+import observables as obs  # noqa: E402
+
+MODELS = {"sl_equal": 1, "sl_double": 2, "sl_quad": 4}
+STAT_LAGS = [1, 2, 5, 10, 20, 50]
+
+
+def run_efpol(ref_bin, seed, L, N, tmax, interval, tmpdir):
+    out = os.path.join(tmpdir, f"run_{L}_{N}_{seed}")
+    subprocess.run([ref_bin, str(seed), out, "1.2", str(tmax), str(interval), str(N), "0", str(L), "sl_equal"],
+                   check=True, stdout=subprocess.DEVNULL)
+    return os.path.join(out, f"N_{N}")
+
+
+def stats_of_run(d, tmax, interval, L, therm):
+    rg, sl, hist, cms = [], [], None, []
+    for t in range(0, tmax + 1, interval):
+        with open(os.path.join(d, f"t={t}_dev=0.res")) as f:
+            _, start, bonds = obs.parse_tuv(f.read())
+        r, _, s = obs.chain_stats(start, bonds)
+        cms.append(obs.cms_tuv(start, bonds))
+        if t >= therm:
+            rg.append(r.mean())
+            sl.append(s.mean())
+            h = obs.run_length_hist(bonds)
+            hist = h if hist is None else hist + h
+    cms_t = obs.unwrap_series(np.array(cms), L)[therm // interval:]
+    msd = obs.cms_msd(cms_t, STAT_LAGS)
+    return float(np.mean(rg)), float(np.mean(sl)), (hist / hist.sum()).tolist(), msd.tolist()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={args.ref}"], check=True,
+                   stdout=subprocess.DEVNULL)
+    refdir = os.path.join(REPO, "oracle", "_ref")
+    efpol = os.path.join(refdir, "efpol_ring")
+    tmp = tempfile.mkdtemp(prefix="elp_golden_")
+    try:
+        for name, code in MODELS.items():
+            raw = os.path.join(tmp, f"tab_{name}.bin")
+            subprocess.run([os.path.join(refdir, "ref_table_dump_ring"), str(code), "5", raw], check=True)
+            a = np.fromfile(raw, dtype=np.uint32)
+            np.savez_compressed(os.path.join(HERE, f"table_{name}.npz"), trans=a[:4096],
+                                add_occ=a[4096:8192].astype(np.int32), rem_occ=a[8192:].astype(np.int32))
+
+        d = run_efpol(efpol, 1, 32, 100, 200, 100, tmp)
+        for t in (0, 100, 200):
+            with open(os.path.join(d, f"t={t}_dev=0.res"), "rb") as f, \
+                    gzip.GzipFile(os.path.join(HERE, f"efpol_L32_N100_s1_t{t}.res.gz"), "wb", mtime=0) as g:
+                g.write(f.read())
+
+        d = run_efpol(efpol, 3, 16, 50, 100, 10, tmp)
+        for t in range(0, 101, 10):
+            with open(os.path.join(d, f"t={t}_dev=0.res"), "rb") as f, \
+                    gzip.GzipFile(os.path.join(HERE, f"efpol_L16_N50_s3_t{t}.res.gz"), "wb", mtime=0) as g:
+                g.write(f.read())
+
+        for (L, N, tmax, interval, therm, seeds) in [(16, 50, 20000, 100, 2000, range(11, 19)),
+                                                      (32, 100, 10000, 100, 3000, range(21, 25))]:
+            per_seed = []
+            for s in seeds:
+                d = run_efpol(efpol, s, L, N, tmax, interval, tmp)
+                rg, sl, hist, msd = stats_of_run(d, tmax, interval, L, therm)
+                per_seed.append({"seed": s, "rg2": rg, "sl_frac": sl, "run_hist": hist, "msd": msd})
+                shutil.rmtree(os.path.dirname(d))
+            out = {"engine": "reference efpol_ring (cpupol, sl_equal), built from source",
+                   "L": L, "N": N, "density": 1.2, "steps": tmax, "interval": interval, "therm": therm,
+                   "msd_lags_intervals": STAT_LAGS, "per_seed": per_seed}
+            with open(os.path.join(HERE, f"efpol_stats_L{L}_N{N}.json"), "w") as f:
+                json.dump(out, f, indent=1)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,184 @@
+"""Bit-exact parity of the sm_100a sweep kernel with the host replay.
+
+The replay (oracle/replay.c) applies the same schedule -- origin shifts,
+colours, anchors, Philox counters -- on the CPU; the GPU state (every site
+word and every chain record) must equal it after every step.  The replay is in
+turn tied to the reference: its initial states are the reference's t=0
+configurations and its statistics match reference efpol (test_gpu_stats.py).
+"""
+import gzip
+import os
+
+import numpy as np
+import pytest
+
+import elp
+import observables as obs
+from oracle_binding import Efpol, Replay
+
+pytestmark = pytest.mark.gpu
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(REPO, "tests", "golden")
+
+
+def replay_for(m: elp.Melt, seed, salt=0):
+    i = m.info()
+    return Replay(i.L, i.N, i.P, seed=seed, salt=salt, periodic=bool(i.periodic),
+                  tile=tuple(i.tile), ncol=i.ncol)
+
+
+def efpol_start(L, N, P):
+    e = Efpol(L, N, P, 0)
+    e.create()
+    return e.export()
+
+
+CASES = [
+    # (L, N, kwargs, steps)
+    (16, 50, dict(), 12),                                   # whole box, 16 colours
+    (32, 100, dict(), 6),                                   # the plain L=32 melt, whole box
+    (24, 60, dict(), 6),                                    # whole box, 24 colours
+    (32, 100, dict(periodic=0, tile=(16, 16, 16)), 8),      # tiled with origin shifts
+    (64, 200, dict(periodic=0, tile=(32, 32, 32)), 3),
+    (48, 100, dict(periodic=0, tile=(48, 24, 24)), 3),
+    (32, 50, dict(periodic=0, tile=(32, 16, 8)), 6),
+]
+
+
+@pytest.mark.parametrize("L,N,kw,steps", CASES)
+def test_kernel_matches_replay_every_step(L, N, kw, steps):
+    seed = 1000 + L + N
+    m = elp.Melt(L=L, N=N, seed=seed, **kw)
+    m.init_melt()
+    r = replay_for(m, seed)
+    start, bonds = efpol_start(L, N, m.P)
+    assert r.load(start, bonds) == 0
+    w, rec = m.state()
+    assert np.array_equal(w, r.lattice()) and np.array_equal(rec, r.records())
+    for s in range(steps):
+        m.run(1)
+        r.steps(1)
+        w, rec = m.state()
+        assert np.array_equal(w, r.lattice()), f"site words differ after step {s + 1}"
+        assert np.array_equal(rec, r.records()), f"records differ after step {s + 1}"
+    assert m.check() == 0
+    assert m.accepted() == r.accepted
+
+
+def test_multi_step_launches_equal_single_steps():
+    a = elp.Melt(L=16, N=50, seed=9, steps_per_launch=1)
+    b = elp.Melt(L=16, N=50, seed=9, steps_per_launch=25)
+    a.init_melt()
+    b.init_melt()
+    a.run(50)
+    b.run(50)
+    wa, ra = a.state()
+    wb, rb = b.state()
+    assert np.array_equal(wa, wb) and np.array_equal(ra, rb)
+
+
+def test_initial_melt_is_reference_t0(tmp_path):
+    m = elp.Melt(L=32, N=100, seed=1)
+    m.init_melt()
+    p = str(tmp_path / "t=0_dev=0.res")
+    m.write_tuv(p)
+    ref = gzip.open(os.path.join(GOLD, "efpol_L32_N100_s1_t0.res.gz"), "rt").read()
+    assert open(p).read() == ref
+
+
+def test_chains_roundtrip_through_device():
+    text = gzip.open(os.path.join(GOLD, "efpol_L16_N50_s3_t100.res.gz"), "rt").read()
+    L, start, bonds = obs.parse_tuv(text)
+    m = elp.Melt(L=16, N=50, seed=3)
+    m.load_chains(start, bonds)
+    s2, b2 = m.fetch()
+    assert np.array_equal(s2, start) and np.array_equal(b2, bonds)
+    assert m.check() == 0
+
+
+def test_resume_from_tuv_is_bit_identical(tmp_path):
+    """A run stopped at a dump and resumed from the TUV file (with its step
+    count) continues the same trajectory: the counter RNG is keyed by the
+    absolute step."""
+    a = elp.Melt(L=32, N=100, seed=5, periodic=0, tile=(16, 16, 16))
+    a.init_melt()
+    a.run(40)
+    b = elp.Melt(L=32, N=100, seed=5, periodic=0, tile=(16, 16, 16))
+    b.init_melt()
+    b.run(17)
+    p = str(tmp_path / "t=17_dev=0.res")
+    b.write_tuv(p)
+    c = elp.Melt(L=32, N=100, seed=5, periodic=0, tile=(16, 16, 16))
+    c.load_tuv(p, step=17)
+    c.run(23)
+    wa, ra = a.state()
+    wc, rc = c.state()
+    assert np.array_equal(wa, wc) and np.array_equal(ra, rc)
+
+
+def test_invariants_hold_over_a_long_run():
+    m = elp.Melt(L=32, N=100, seed=77)
+    m.init_melt()
+    for _ in range(20):
+        m.run(50)
+        assert m.check() == 0
+    start, bonds = m.fetch()
+    e = Efpol(32, 100, m.P, 0)
+    assert e.read(obs.format_tuv(32, start, bonds)) == 0
+    assert e.check() == 0          # the reference's own integrity rules, restated
+
+
+def test_large_box_invariants_and_conservation():
+    """The L=256, N=5000 melt (20.1 M monomers): a few steps keep every
+    invariant; the monomer total is conserved."""
+    m = elp.Melt(L=256, N=5000, seed=11)
+    assert m.P == 4027
+    m.init_melt()
+    m.run(3)
+    assert m.check() == 0
+    w, rec = m.state()
+    counts = np.where(w & 16, 0, w >> 5).astype(np.int64).sum() + rec[:, 1].astype(np.int64).sum()
+    assert counts == 5000 * 4027
+
+
+def test_l128_matches_replay():
+    """The single large melt L=128, N=1000 (2517 rings), default geometry."""
+    m = elp.Melt(L=128, N=1000, seed=7)
+    assert m.P == 2517
+    m.init_melt()
+    r = replay_for(m, 7)
+    assert r.load(*efpol_start(128, 1000, m.P)) == 0
+    for _ in range(2):
+        m.run(1)
+        r.steps(1)
+    w, rec = m.state()
+    assert np.array_equal(w, r.lattice()) and np.array_equal(rec, r.records())
+
+
+def test_bad_inputs_fail_cleanly(tmp_path):
+    m = elp.Melt(L=16, N=50, seed=1)
+    with pytest.raises(elp.ElpError) as e:
+        m.run(1)                                   # nothing loaded yet
+    assert e.value.status == elp.ERR_STATE
+    with pytest.raises(elp.ElpError) as e:
+        m.load_tuv(str(tmp_path / "missing.res"))
+    assert e.value.status == elp.ERR_IO
+    text = gzip.open(os.path.join(GOLD, "efpol_L16_N50_s3_t100.res.gz"), "rt").read()
+    p = tmp_path / "garbled.res"
+    p.write_text(text[: len(text) // 2] + "zz")
+    with pytest.raises(elp.ElpError) as e:
+        m.load_tuv(str(p))
+    assert e.value.status == elp.ERR_FORMAT
+    L, start, bonds = obs.parse_tuv(text)
+    bad = bonds.copy()
+    bad[3, int(np.flatnonzero(bad[3])[0])] = 0x3   # not a lattice bond
+    with pytest.raises(elp.ElpError) as e:
+        m.load_chains(start, bad)
+    assert e.value.status == elp.ERR_INTEGRITY
+    clash = start.copy()
+    clash[1] = clash[0]                            # two rings on one site
+    b2 = bonds.copy()
+    b2[1] = b2[0]
+    with pytest.raises(elp.ElpError) as e:
+        m.load_chains(clash, b2)
+    assert e.value.status == elp.ERR_INTEGRITY
