@@ -56,6 +56,7 @@ typedef struct elp_job_spec {
     int32_t ncol;             /* colour modulus, 0 = auto */
     int32_t device;           /* CUDA device ordinal */
     int32_t steps_per_launch; /* whole-box domains: steps per kernel launch (>=1) */
+    int32_t kernel;           /* 0 auto (specialised when the shape has one), 1 generic */
 } elp_job_spec;
 
 typedef struct elp_info {

@@ -43,6 +43,8 @@ struct elp_ctx {
     int device;
     int spl;                       // steps per launch (whole-box domains)
     int domains, threads;
+    int nsm;                       // SMs of the device
+    int generic;                   // force the generic kernel
     cudaStream_t stream;
     cudaEvent_t ev0, ev1;
     uint32_t* d_lat;
@@ -57,6 +59,19 @@ struct elp_ctx {
     size_t device_bytes;
     int loaded;
 };
+
+// Device-side error flags (set by kernels instead of trapping); read after a
+// stream synchronisation.
+static elp_status device_errors(elp_ctx* c)
+{
+    uint32_t flags = 0;
+    CUDA_TRY(cudaMemcpyAsync(&flags, c->d_acc + 1, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (flags & 1u)
+        return fail(ELP_ERR_STATE, "a domain held more monomer-0 runs than its label table; steps after the "
+                                   "overflow are incomplete (use the generic kernel for this melt)");
+    return ELP_OK;
+}
 
 extern "C" void elp_default_spec(elp_job_spec* s)
 {
@@ -105,7 +120,7 @@ extern "C" elp_status elp_create(const elp_job_spec* spec, elp_ctx** out)
     if (!spec || !out) return fail(ELP_ERR_ARG, "null argument");
     *out = nullptr;
     if (spec->L < 5 || spec->L > 1024) return fail(ELP_ERR_ARG, "box edge L=%d out of range [5,1024]", spec->L);
-    if (spec->N < 3) return fail(ELP_ERR_ARG, "ring length N=%d < 3", spec->N);
+    if (spec->N < 3 || spec->N > ELP_MAX_N) return fail(ELP_ERR_ARG, "ring length N=%d outside [3,%d]", spec->N, ELP_MAX_N);
     int P = spec->P > 0 ? spec->P : elp_get_npol(spec->density, spec->N, (long)spec->L * spec->L * spec->L);
     if (P < 1) P = 1;
     if ((long)P >= (1L << 27)) return fail(ELP_ERR_ARG, "too many rings (%d)", P);
@@ -131,6 +146,9 @@ extern "C" elp_status elp_create(const elp_job_spec* spec, elp_ctx** out)
     c->salt = spec->salt;
     c->device = spec->device;
     c->spl = spec->steps_per_launch > 0 ? spec->steps_per_launch : 1;
+    c->generic = spec->kernel == 1;
+    if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, spec->device) != cudaSuccess || c->nsm < 1)
+        c->nsm = 148;
     c->domains = g.periodic ? 1 : (g.L / g.tx) * (g.L / g.ty) * (g.L / g.tz);
     c->threads = (c->lay.groups + 31) / 32 * 32;
     if (c->threads < 32) c->threads = 32;
@@ -230,7 +248,7 @@ extern "C" elp_status elp_get_state(elp_ctx* c, uint32_t* words, uint32_t* recor
     CUDA_TRY(cudaMemcpyAsync(words, c->d_lat, S * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaMemcpyAsync(records, c->d_rec, (size_t)c->P * ELP_REC_WORDS * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return ELP_OK;
+    return device_errors(c);
 }
 
 static elp_status enqueue_steps(elp_ctx* c, int64_t nsteps)
@@ -240,6 +258,8 @@ static elp_status enqueue_steps(elp_ctx* c, int64_t nsteps)
     a.rec = c->d_rec;
     a.table = c->d_table;
     a.accepted = c->d_acc;
+    a.error = reinterpret_cast<uint32_t*>(c->d_acc + 1);
+    a.nchains = c->P;
     a.L = c->g.L;
     a.periodic = c->g.periodic;
     a.tx = c->g.tx; a.ty = c->g.ty; a.tz = c->g.tz;
@@ -253,7 +273,9 @@ static elp_status enqueue_steps(elp_ctx* c, int64_t nsteps)
         int k = c->g.periodic ? (int)(nsteps < c->spl ? nsteps : c->spl) : 1;
         a.step0 = c->step;
         a.nsteps = k;
-        CUDA_TRY(elp_launch_sweep(&a, c->domains, c->threads, c->lay.bytes, c->stream));
+        cudaError_t e = c->generic ? cudaErrorNotSupported : elp_launch_sweep2(&a, c->nsm, c->stream);
+        if (e == cudaErrorNotSupported) e = elp_launch_sweep(&a, c->domains, c->threads, c->lay.bytes, c->stream);
+        CUDA_TRY(e);
         c->step += (uint64_t)k;
         nsteps -= k;
     }
@@ -281,7 +303,7 @@ extern "C" elp_status elp_run_timed(elp_ctx* c, int64_t nsteps, float* ms)
     CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
     CUDA_TRY(cudaEventSynchronize(c->ev1));
     CUDA_TRY(cudaEventElapsedTime(ms, c->ev0, c->ev1));
-    return ELP_OK;
+    return device_errors(c);
 }
 
 extern "C" elp_status elp_sync(elp_ctx* c)
@@ -289,7 +311,7 @@ extern "C" elp_status elp_sync(elp_ctx* c)
     if (!c) return fail(ELP_ERR_ARG, "null context");
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return ELP_OK;
+    return device_errors(c);
 }
 
 extern "C" elp_status elp_accepted(elp_ctx* c, uint64_t* acc)
@@ -333,6 +355,8 @@ extern "C" elp_status elp_fetch_chains(elp_ctx* c, int32_t* start, uint8_t* bond
     CUDA_TRY(cudaMemcpyAsync(bonds, c->d_bonds, (size_t)c->P * c->N, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaMemcpyAsync(status.data(), c->d_status, (size_t)c->P * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    elp_status dev = device_errors(c);
+    if (dev) return dev;
     for (int p = 0; p < c->P; p++)
         if (status[(size_t)p]) return fail(ELP_ERR_INTEGRITY, "ring %d cannot be walked (code %d)", p, status[(size_t)p]);
     return ELP_OK;
@@ -361,6 +385,8 @@ extern "C" elp_status elp_check(elp_ctx* c, int32_t* code)
     CUDA_TRY(cudaMemcpyAsync(status.data(), c->d_status, (size_t)c->P * 4, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaMemcpyAsync(cnt, c->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    elp_status dev = device_errors(c);
+    if (dev) return dev;
     int rc = 0;
     for (int p = 0; p < c->P && !rc; p++)
         if (status[(size_t)p]) rc = 4;

@@ -63,12 +63,12 @@ __device__ __forceinline__ uint32_t global_site(const Dom& D, int p)
 
 __device__ __forceinline__ uint32_t run_len(const Dom& D, uint32_t w)
 {
-    return (w & ELP_LBIT) ? D.rec[ELP_REC_WORDS * (w >> 5) + 1] : (w >> 5);
+    return (w & ELP_LBIT) ? D.rec[ELP_REC_WORDS * (w >> 5) + 1] : (w >> ELP_CSHIFT);
 }
 
 // General form of the move, including the bookkeeping of monomer 0's run.
 // Taken only when a labelled run is involved (about one site per chain).
-__device__ __noinline__ int op_slow(const Dom& D, int p, const int* off, uint32_t s, uint32_t r4)
+static __device__ __noinline__ int op_slow(const Dom& D, int p, const int* off, uint32_t s, uint32_t r4)
 {
     uint32_t* S = D.S;
     uint32_t wP = S[p];
@@ -97,11 +97,11 @@ __device__ __noinline__ int op_slow(const Dom& D, int p, const int* off, uint32_
     uint32_t cN = d2 ? 0 : run_len(D, wY);
 
     uint32_t nPc = cP + (d1 == 0) - (src1 == 0);
-    uint32_t wP2 = (d1 ? d1 : d2) | (nPc << 5);
+    uint32_t wP2 = (d1 ? d1 : d2) | (nPc << ELP_CSHIFT);
     uint32_t wB2 = 0, wY2 = 0;
-    if (s == 1 && src2 == 0) wB2 = (wB & 15) | ((cB - 1) << 5);
-    if (d1 && d2) wY2 = d2 | (1u << 5);
-    else if (!d2) wY2 = (wY & 15) | ((cN + 1) << 5);
+    if (s == 1 && src2 == 0) wB2 = (wB & 15) | ((cB - 1) << ELP_CSHIFT);
+    if (d1 && d2) wY2 = d2 | ELP_CUNIT;
+    else if (!d2) wY2 = (wY & 15) | ((cN + 1) << ELP_CSHIFT);
 
     int lab = -1;
     uint32_t chain = 0;
@@ -124,7 +124,7 @@ __device__ __noinline__ int op_slow(const Dom& D, int p, const int* off, uint32_
         uint32_t* tgt = nl == 0 ? &wP2 : (nl == 1 ? &wB2 : &wY2);
         int ps = nl == 0 ? p : (nl == 1 ? pB : pY);
         rc[0] = global_site(D, ps);
-        rc[1] = *tgt >> 5;
+        rc[1] = *tgt >> ELP_CSHIFT;
         rc[2] = noff;
         *tgt = (*tgt & 15) | ELP_LBIT | (chain << 5);
     }
@@ -148,7 +148,7 @@ __device__ __forceinline__ int op(const Dom& D, int p, const int* off, uint32_t 
     int pB = 0;
     uint32_t lab = wP & ELP_LBIT;
     if (s == 0) {
-        if (!lab && wP < (2u << 5)) return 0;
+        if (!lab && wP < 2u * ELP_CUNIT) return 0;
         src1 = 0;
         src2 = bo;
     } else {
@@ -157,7 +157,7 @@ __device__ __forceinline__ int op(const Dom& D, int p, const int* off, uint32_t 
         if (wB == ELP_WALL) return 0;
         lab |= wB & ELP_LBIT;
         src1 = bo;
-        src2 = (wB >= (2u << 5)) ? 0 : (wB & 15);
+        src2 = (wB >= 2u * ELP_CUNIT) ? 0 : (wB & 15);
     }
     if (lab) return op_slow(D, p, off, s, r4);
     uint32_t e = D.tab[(src1 << 8) | (src2 << 4) | r4];
@@ -171,11 +171,11 @@ __device__ __forceinline__ int op(const Dom& D, int p, const int* off, uint32_t 
         if (wY == ELP_WALL) return 0;
         if (wY & ELP_LBIT) return op_slow(D, p, off, s, r4);
     }
-    uint32_t cw = wP & ~31u;
-    cw = (s == 0) ? cw - 32u : (d1 ? cw : cw + 32u);
+    uint32_t cw = wP & ~15u;
+    cw = (s == 0) ? cw - ELP_CUNIT : (d1 ? cw : cw + ELP_CUNIT);
     S[p] = cw | (d1 ? d1 : d2);
-    if (s) S[pB] = (src2 == 0) ? wB - 32u : 0u;
-    if (d1) S[pY] = d2 ? (d2 | 32u) : wY + 32u;
+    if (s) S[pB] = (src2 == 0) ? wB - ELP_CUNIT : 0u;
+    if (d1) S[pY] = d2 ? (d2 | ELP_CUNIT) : wY + ELP_CUNIT;
     return 1;
 }
 

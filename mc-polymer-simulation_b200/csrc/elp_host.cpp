@@ -268,7 +268,7 @@ int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t
                 rec[ELP_REC_WORDS * p + 2] = (uint32_t)off0;
                 rec[ELP_REC_WORDS * p + 3] = 0;
             } else {
-                lat[site] = bo | ((uint32_t)len << 5);
+                lat[site] = bo | ((uint32_t)len << ELP_CSHIFT);
             }
             done += len;
             m = (m + len) % N;

@@ -4,8 +4,12 @@
 //   bits 0-3   b_out: FCC bond code from the last monomer of the run on this
 //              site to the next site of its chain (0 only on empty sites)
 //   bit  4     label: the run holds monomer 0 of its chain
-//   bits 5-31  run length (label clear) or chain id (label set)
+//   label clear: bits 16-31 run length, bits 5-15 zero
+//   label set:   bits 5-31 chain id; the run length is in the chain record
 //   0          empty site
+// (Inside the specialised sweep kernels a labelled word is rewritten while its
+// tile is on chip: bits 5-15 index a shared-memory label slot and bits 16-31
+// hold the run length, so every on-chip word carries its count.)
 // Chain record (4 x uint32 per chain): {global site of monomer 0's run,
 //   length of that run, offset of monomer 0 inside it, unused}.
 //
@@ -16,6 +20,9 @@
 #include <stddef.h>
 
 #define ELP_LBIT 16u
+#define ELP_CSHIFT 16            // run length position
+#define ELP_CUNIT (1u << 16)     // +1 monomer in a run
+#define ELP_MAX_N 65536          // longest ring (run lengths fit 16 bits)
 #define ELP_WALL 0xFFFFFFFFu
 #define ELP_REC_WORDS 4
 

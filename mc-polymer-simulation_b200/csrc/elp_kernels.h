@@ -8,6 +8,8 @@ struct SweepArgs {
     uint32_t* rec;                 // chain records
     const uint32_t* table;         // 1024 words = 4096 bytes dst1|dst2<<4
     unsigned long long* accepted;  // optional accepted-move counter
+    uint32_t* error;               // device error flags (bit 0: label slot table overflow)
+    int nchains;                   // rings in the melt
     int L, periodic, tx, ty, tz, ncol;
     int sx, sxy, ox, words, groups;
     uint32_t seed, salt;
@@ -28,6 +30,7 @@ struct WalkArgs {
 
 extern "C" {
 cudaError_t elp_launch_sweep(const SweepArgs* a, int ndomains, int threads, size_t smem, cudaStream_t s);
+cudaError_t elp_launch_sweep2(const SweepArgs* a, int nsm, cudaStream_t s);
 cudaError_t elp_launch_walk(const WalkArgs* a, cudaStream_t s);
 cudaError_t elp_launch_scan(const WalkArgs* a, cudaStream_t s);
 }

@@ -1,0 +1,342 @@
+// elp_sweep2.cu -- specialised sweep kernels for the common domain shapes.
+//
+// Same schedule and results as the generic sweep_kernel (elp_sweep.cu); what
+// changes is how the work is fed to the SM:
+//   * tile edges and shared-memory strides are compile-time constants;
+//   * the four anchors a thread owns in a substep are processed stage by
+//     stage (all first loads, then all second loads, ...), so the dependent
+//     shared-memory loads of four independent moves overlap;
+//   * monomer 0's runs are handled inline: while a tile is on chip each
+//     labelled word carries its run length (bits 16-31) and a slot number
+//     (bits 5-15) into a small shared-memory table {chain, offset, site};
+//     the chain records in global memory are read when the tile is loaded and
+//     written back when it is stored, so no move waits on global memory;
+//   * tiles are fetched with cp.async (4-byte granules: the origin shift
+//     makes rows unaligned) and the grid is persistent over the tiles.
+#include <cuda_runtime.h>
+
+#include "elp_device.cuh"
+#include "elp_kernels.h"
+
+namespace elp {
+
+__device__ __forceinline__ void cp_async4(uint32_t* sdst, const uint32_t* gsrc)
+{
+    uint32_t s = (uint32_t)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP>
+struct Shape {
+    static constexpr int R = TY * TZ;
+    static constexpr int A = R * (TX / NC);
+    static constexpr int G = A / 4;
+    static constexpr int HALO = PER ? 0 : 2;
+    static constexpr int OX = PER ? 0 : 1 + SX + SXY;
+    static constexpr int WORDS = SXY * (TZ + HALO);
+    static constexpr int SITES = TX * TY * TZ;
+    static constexpr size_t BYTES = (size_t)WORDS * 4 + 4096 + 27 * 16 * 4 + 64 * 4 + (size_t)CAP * 12 + 16;
+};
+
+constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
+
+// Four anchors of one thread, one substep.  Returns accepted moves.
+template <bool PER, int NC>
+__device__ __forceinline__ int substep4(uint32_t* S, const uint8_t* tab, const int* offs, uint32_t* slot_off,
+                                        int* slot_site, const int (&base)[4], const int (&rot)[4],
+                                        const int (&clsyz)[4], const int (&xj)[4], int c, uint32_t w, int L)
+{
+    int p[4];
+    const int* off[4];
+    uint32_t wP[4], rb[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int xr = c + rot[q];
+        xr -= xr >= NC ? NC : 0;
+        p[q] = base[q] + xr;
+        int cls = clsyz[q];
+        if (PER) {
+            int x = xr + xj[q];
+            cls += x == 0 ? 0 : (x == L - 1 ? 2 : 1);
+        }
+        off[q] = offs + 16 * cls;
+        wP[q] = S[p[q]];
+        rb[q] = (w >> (8 * q)) & 0xffu;
+    }
+    // stage B: the next run (slot 1)
+    int pB[4];
+    uint32_t wB[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        pB[q] = p[q] + off[q][wP[q] & 15];
+        wB[q] = ((rb[q] & 1) && wP[q]) ? S[pB[q]] : 0u;
+    }
+    // stage C: source bonds (b_{m-1}, b_m) and the table option
+    uint32_t e[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint32_t s = rb[q] & 1, bo = wP[q] & 15;
+        const bool live = wP[q] != 0 && (s ? wB[q] != ELP_WALL : wP[q] >= 2u * ELP_CUNIT);
+        const uint32_t src2 = s ? ((wB[q] >= 2u * ELP_CUNIT) ? 0u : (wB[q] & 15)) : bo;
+        const uint32_t idx = ((s ? bo : 0u) << 8) | (src2 << 4) | ((rb[q] >> 1) & 15);
+        e[q] = live ? (uint32_t)tab[idx] : 0u;
+    }
+    // stage D: target site P + dst1
+    int pY[4];
+    uint32_t wY[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        pY[q] = p[q] + off[q][e[q] & 15];
+        wY[q] = e[q] ? S[pY[q]] : 0u;
+    }
+    // stage E: accept, label bookkeeping, write
+    int acc = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint32_t d1 = e[q] & 15, d2 = e[q] >> 4, s = rb[q] & 1;
+        const bool join = d2 == 0;  // m joins the front of the next run
+        const bool ok = e[q] && (join ? wY[q] != ELP_WALL : (d1 == 0 || wY[q] == 0));
+        uint32_t nP = wP[q] & ~15u;
+        nP = (s == 0) ? nP - ELP_CUNIT : (d1 ? nP : nP + ELP_CUNIT);
+        nP |= d1 ? d1 : d2;
+        uint32_t nB = (wB[q] >= 2u * ELP_CUNIT) ? wB[q] - ELP_CUNIT : 0u;
+        uint32_t nY = d2 ? (d2 | ELP_CUNIT) : wY[q] + ELP_CUNIT;
+        const uint32_t labs = (wP[q] | (s ? wB[q] : 0u) | (join ? wY[q] : 0u)) & ELP_LBIT;
+        if (ok && labs) {
+            // monomer 0 sits in one of the runs this move touches
+            const int src = (wP[q] & ELP_LBIT) ? 0 : ((s && (wB[q] & ELP_LBIT)) ? 1 : 2);
+            const uint32_t lw = src == 0 ? wP[q] : (src == 1 ? wB[q] : wY[q]);
+            const uint32_t slot = (lw >> 5) & 0x7FFu;
+            const uint32_t off0 = slot_off[slot];
+            uint32_t noff;
+            int nl;
+            if (src == 0) {
+                nl = 0; noff = off0;
+                if (s == 0 && off0 == (wP[q] >> ELP_CSHIFT) - 1) { nl = 2; noff = 0; }
+            } else if (src == 1) {
+                if (wB[q] >= 2u * ELP_CUNIT && off0 > 0) { nl = 1; noff = off0 - 1; }
+                else { nl = d1 ? 2 : 0; noff = d1 ? 0 : (nP >> ELP_CSHIFT) - 1; }
+            } else {
+                nl = 2; noff = off0 + 1;
+            }
+            const uint32_t lb = lw & LMASK;
+            if (src == 0) nP &= ~LMASK; else if (src == 1) nB &= ~LMASK; else nY &= ~LMASK;
+            if (nl == 0) nP |= lb; else if (nl == 1) nB |= lb; else nY |= lb;
+            slot_off[slot] = noff;
+            slot_site[slot] = nl == 0 ? p[q] : (nl == 1 ? pB[q] : pY[q]);
+        }
+        if (ok) S[p[q]] = nP;
+        if (ok && s) S[pB[q]] = nB;
+        if (ok && d1) S[pY[q]] = nY;
+        acc += ok ? 1 : 0;
+    }
+    return acc;
+}
+
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
+{
+    using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP>;
+    static_assert(SH::G <= THREADS, "threads");
+    static_assert(CAP <= 2048, "slot numbers are 11 bits");
+    extern __shared__ __align__(16) uint32_t smem[];
+    uint32_t* S = smem;
+    uint8_t* tab = reinterpret_cast<uint8_t*>(smem + SH::WORDS);
+    int* offs = reinterpret_cast<int*>(tab + 4096);
+    uint32_t* col = reinterpret_cast<uint32_t*>(offs + 27 * 16);
+    uint32_t* slot_chain = col + 64;
+    uint32_t* slot_off = slot_chain + CAP;
+    int* slot_site = reinterpret_cast<int*>(slot_off + CAP);
+    uint32_t* nslots = reinterpret_cast<uint32_t*>(slot_site + CAP);
+    const int tid = threadIdx.x;
+    const int L = a.L;
+    const uint2 key = make_uint2(a.seed, a.salt);
+
+    for (int i = tid; i < 1024; i += THREADS) reinterpret_cast<uint32_t*>(tab)[i] = a.table[i];
+    for (int i = tid; i < 27 * 16; i += THREADS) {
+        int cls = i >> 4, b = i & 15;
+        int dt = elp_bt(b), du = elp_bu(b), dv = elp_bv(b);
+        if (PER) {
+            int cx = cls % 3, cy = (cls / 3) % 3, cz = cls / 9;
+            if (cx == 0 && dt < 0) dt = L - 1;
+            if (cx == 2 && dt > 0) dt = -(L - 1);
+            if (cy == 0 && du < 0) du = L - 1;
+            if (cy == 2 && du > 0) du = -(L - 1);
+            if (cz == 0 && dv < 0) dv = L - 1;
+            if (cz == 2 && dv > 0) dv = -(L - 1);
+        }
+        offs[i] = dt + SX * du + SXY * dv;
+    }
+    if (!PER)
+        for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = ELP_WALL;
+
+    int base[4], rot[4], clsyz[4], xj[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int an = tid + q * SH::G;
+        int j = an / SH::R, row = an % SH::R;
+        int y = row % TY, z = row / TY;
+        int m = (2 * y + 3 * z) % NC;
+        rot[q] = m ? NC - m : 0;
+        base[q] = SH::OX + SX * y + SXY * z + NC * j;
+        int cy = y == 0 ? 0 : (y == L - 1 ? 2 : 1);
+        int cz = z == 0 ? 0 : (z == L - 1 ? 2 : 1);
+        clsyz[q] = PER ? (3 * cy + 9 * cz) : 13;
+        xj[q] = NC * j;
+    }
+    const bool active = tid < SH::G;
+
+    Dom D;
+    D.S = S; D.tab = tab; D.rec = a.rec;
+    D.ox = SH::OX; D.sx = SX; D.sxy = SXY; D.L = L;
+    D.x0 = 0; D.y0 = 0; D.z0 = 0;
+
+    const int ntx = L / TX, nty = L / TY, ntz = L / TZ;
+    const int ntiles = PER ? 1 : ntx * nty * ntz;
+    int accepted = 0;
+
+    for (int st = 0; st < a.nsteps; st++) {
+        const uint32_t t = (uint32_t)(a.step0 + st);
+        int sh0 = 0, sh1 = 0, sh2 = 0;
+        if (!PER) {
+            uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
+            sh0 = (int)bounded(sh.x, TX); sh1 = (int)bounded(sh.y, TY); sh2 = (int)bounded(sh.z, TZ);
+        }
+        bool overflow = false;
+        for (int d = blockIdx.x; d < ntiles; d += gridDim.x) {
+            if (!PER) {
+                D.x0 = sh0 + (d % ntx) * TX;
+                D.y0 = sh1 + ((d / ntx) % nty) * TY;
+                D.z0 = sh2 + (d / ntx / nty) * TZ;
+            }
+            if (!PER || st == 0) {
+                __syncthreads();  // the previous tile's stores have read shared memory
+                if (tid == 0) *nslots = 0;
+                for (int i = tid; i < SH::SITES; i += THREADS) {
+                    int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
+                    int gx = D.x0 + x; gx -= gx >= L ? L : 0;
+                    int gy = D.y0 + y; gy -= gy >= L ? L : 0;
+                    int gz = D.z0 + z; gz -= gz >= L ? L : 0;
+                    cp_async4(S + SH::OX + x + SX * y + SXY * z,
+                              a.lat + (size_t)gx + (size_t)L * ((size_t)gy + (size_t)L * gz));
+                }
+                cp_async_wait_all();
+                __syncthreads();
+                // monomer-0 runs: global chain id -> shared slot, run length inline
+                for (int i = tid; i < SH::SITES; i += THREADS) {
+                    int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
+                    int idx = SH::OX + x + SX * y + SXY * z;
+                    uint32_t wv = S[idx];
+                    if (wv & ELP_LBIT) {
+                        uint32_t slot = atomicAdd(nslots, 1u);
+                        uint32_t chain = wv >> 5;
+                        if (slot < (uint32_t)CAP) {
+                            uint4 r = *reinterpret_cast<const uint4*>(a.rec + ELP_REC_WORDS * (size_t)chain);
+                            slot_chain[slot] = chain;
+                            slot_off[slot] = r.z;
+                            slot_site[slot] = idx;
+                            S[idx] = (wv & 15) | ELP_LBIT | (slot << 5) | (r.y << ELP_CSHIFT);
+                        }
+                    }
+                }
+            }
+            if (tid < (2 * NC + 3) / 4) {
+                uint4 cw = philox(make_uint4(t, (uint32_t)d, (uint32_t)tid | ELP_STREAM_COLOUR, 0), key);
+                col[4 * tid + 0] = bounded(cw.x, NC);
+                col[4 * tid + 1] = bounded(cw.y, NC);
+                col[4 * tid + 2] = bounded(cw.z, NC);
+                col[4 * tid + 3] = bounded(cw.w, NC);
+            }
+            __syncthreads();
+            if (*nslots > (uint32_t)CAP) {
+                // more monomer-0 runs than slots: leave this tile untouched, report
+                if (tid == 0) atomicOr(a.error, 1u);
+                overflow = true;
+                continue;
+            }
+
+            uint4 rw = make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+            for (int k = 0; k < 2 * NC; k++) {
+                if (active) {
+                    if ((k & 3) == 0) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                    accepted += substep4<PER, NC>(S, tab, offs, slot_off, slot_site, base, rot, clsyz, xj, (int)col[k],
+                                                  word_of(rw, k & 3), L);
+                }
+                __syncthreads();
+            }
+
+            if (!PER || st == a.nsteps - 1) {
+                const uint32_t ns = *nslots;
+                for (uint32_t sl = tid; sl < ns; sl += THREADS) {
+                    int idx = slot_site[sl];
+                    uint32_t wv = S[idx];
+                    uint32_t chain = slot_chain[sl];
+                    *reinterpret_cast<uint4*>(a.rec + ELP_REC_WORDS * (size_t)chain) =
+                        make_uint4(global_site(D, idx), wv >> ELP_CSHIFT, slot_off[sl], 0u);
+                    S[idx] = (wv & 15) | ELP_LBIT | (chain << 5);
+                }
+                __syncthreads();
+                for (int i = tid; i < SH::SITES; i += THREADS) {
+                    int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
+                    int gx = D.x0 + x; gx -= gx >= L ? L : 0;
+                    int gy = D.y0 + y; gy -= gy >= L ? L : 0;
+                    int gz = D.z0 + z; gz -= gz >= L ? L : 0;
+                    a.lat[(size_t)gx + (size_t)L * ((size_t)gy + (size_t)L * gz)] = S[SH::OX + x + SX * y + SXY * z];
+                }
+            }
+        }
+        if (PER && overflow) break;  // block-uniform: every thread read the same count
+    }
+    if (a.accepted) {
+        unsigned long long v = (unsigned long long)accepted;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0 && v) atomicAdd(a.accepted, v);
+    }
+}
+
+}  // namespace elp
+
+// ---- dispatch ----------------------------------------------------------------
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int THREADS, int MINB>
+static cudaError_t launch2(const SweepArgs* a, int nsm, cudaStream_t s)
+{
+    using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP>;
+    // expected monomer-0 runs per tile must stay well inside the slot table
+    double per_tile = (double)a->nchains * SH::SITES / ((double)a->L * a->L * a->L);
+    if (PER ? a->nchains > CAP : per_tile * 4.0 > CAP) return cudaErrorNotSupported;
+    auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, THREADS, MINB>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    int ntiles = PER ? 1 : (a->L / TX) * (a->L / TY) * (a->L / TZ);
+    int grid = ntiles;
+    if (!PER && grid > nsm * MINB) grid = nsm * MINB;
+    k<<<grid, THREADS, SH::BYTES, s>>>(*a);
+    return cudaGetLastError();
+}
+
+// Returns cudaErrorNotSupported when no specialised kernel fits the job (the
+// caller then uses the generic kernel).
+extern "C" cudaError_t elp_launch_sweep2(const SweepArgs* a, int nsm, cudaStream_t s)
+{
+    if (a->nsteps > 1 && !a->periodic) return cudaErrorNotSupported;
+    if (!a->error) return cudaErrorNotSupported;
+#define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_)                                            \
+    if (a->tx == X_ && a->ty == Y_ && a->tz == Z_ && a->periodic == PER_ && a->ncol == NC_ && a->sx == SX_ &&   \
+        a->sxy == SXY_)                                                                                        \
+        return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_>(a, nsm, s);
+    SHAPE(32, 32, 32, 0, 16, 35, 1190, 1024, 512, 1)
+    SHAPE(32, 32, 16, 0, 16, 35, 1190, 512, 256, 2)
+    SHAPE(16, 16, 16, 0, 16, 19, 342, 256, 64, 4)
+    SHAPE(48, 24, 24, 0, 16, 51, 1326, 1024, 448, 1)
+    SHAPE(16, 16, 16, 1, 16, 16, 256, 2048, 64, 1)
+    SHAPE(32, 32, 32, 1, 16, 33, 1056, 2048, 512, 1)
+    SHAPE(24, 24, 24, 1, 24, 24, 576, 2048, 160, 1)
+#undef SHAPE
+    return cudaErrorNotSupported;
+}

@@ -61,7 +61,7 @@ __global__ void walk_kernel(WalkArgs a)
         if (!wn) { bad = 1; break; }
         if (cur == site) break;
         if (wn & ELP_LBIT) { bad = 1; break; }
-        here = wn >> 5;
+        here = wn >> ELP_CSHIFT;
         if (here == 0 || runs >= (unsigned long long)N) { bad = 1; break; }
     }
     if (!bad && i + (long)off != N) bad = 1;
@@ -89,7 +89,8 @@ __global__ void scan_kernel(WalkArgs a)
             if (ch >= (uint32_t)a.P || a.rec[ELP_REC_WORDS * ch] != (uint32_t)i) { badc++; continue; }
             c = a.rec[ELP_REC_WORDS * ch + 1];
         } else {
-            c = w >> 5;
+            c = w >> ELP_CSHIFT;
+            if (w & 0xFFE0u) badc++;   // bits 5-15 must be clear
         }
         mono += c;
         if (!elp_valid_bond(w & 15) || c == 0 || (a.visit && v == 0)) badc++;

@@ -12,7 +12,8 @@
  *   bits 0-3  b_out: bond from the last monomer of the run on this site to
  *             the next site of the chain (never 0 on an occupied site)
  *   bit  4    label: the run holds monomer 0 of its chain
- *   bits 5-31 run length (unlabelled) or chain id (labelled)
+ *   unlabelled: bits 16-31 run length (bits 5-15 zero)
+ *   labelled:   bits 5-31 chain id, run length in the chain record
  *   word 0    empty site
  * Per chain a record {site of monomer 0's run, its run length, offset of
  * monomer 0 inside that run}.
@@ -37,6 +38,7 @@
 #include <string.h>
 
 #define LBIT 16u
+#define CSH 16
 
 static uint8_t g_tab[4096];
 static int g_tab_ready = 0;
@@ -82,7 +84,7 @@ static inline int dnbr(const dom* D, int x, int y, int z, uint32_t b, int* nx, i
 
 static inline uint32_t w_count(const orc_replay* r, uint32_t w)
 {
-    return (w & LBIT) ? r->rec[4 * (size_t)(w >> 5) + 1] : (w >> 5);
+    return (w & LBIT) ? r->rec[4 * (size_t)(w >> 5) + 1] : (w >> CSH);
 }
 
 /* One anchored move attempt. Returns 1 if the move was applied. */
@@ -121,11 +123,11 @@ static int replay_op(orc_replay* r, const dom* D, int x, int y, int z, uint32_t 
     uint32_t cN = d2 ? 0 : w_count(r, wY);  /* d2 == 0: m joins the next run */
 
     uint32_t nP_c = cP + (d1 == 0) - (src1 == 0);
-    uint32_t wP2 = (d1 ? d1 : d2) | (nP_c << 5);
+    uint32_t wP2 = (d1 ? d1 : d2) | (nP_c << CSH);
     uint32_t wB2 = 0, wY2 = 0;
-    if (s == 1 && src2 == 0) wB2 = (wB & 15) | ((cB - 1) << 5);
-    if (d1 && d2) wY2 = d2 | (1u << 5);
-    else if (!d2) wY2 = (wY & 15) | ((cN + 1) << 5);
+    if (s == 1 && src2 == 0) wB2 = (wB & 15) | ((cB - 1) << CSH);
+    if (d1 && d2) wY2 = d2 | (1u << CSH);
+    else if (!d2) wY2 = (wY & 15) | ((cN + 1) << CSH);
 
     /* monomer-0 label follows its monomer */
     int lab = -1, nl = -1;
@@ -147,7 +149,7 @@ static int replay_op(orc_replay* r, const dom* D, int x, int y, int z, uint32_t 
         uint32_t* tgt = nl == 0 ? &wP2 : (nl == 1 ? &wB2 : &wY2);
         size_t site = nl == 0 ? iP : (nl == 1 ? iB : iY);
         r->rec[4 * (size_t)chain + 0] = (uint32_t)site;
-        r->rec[4 * (size_t)chain + 1] = *tgt >> 5;
+        r->rec[4 * (size_t)chain + 1] = *tgt >> CSH;
         r->rec[4 * (size_t)chain + 2] = noff;
         *tgt = (*tgt & 15) | LBIT | (chain << 5);
     }
@@ -220,7 +222,7 @@ int orc_replay_load(orc_replay* r, const int32_t* start, const uint8_t* bonds)
                 r->rec[4 * (size_t)p + 1] = (uint32_t)len;
                 r->rec[4 * (size_t)p + 2] = (uint32_t)((0 - m + N) % N);
             } else {
-                r->lat[site] = bo | ((uint32_t)len << 5);
+                r->lat[site] = bo | ((uint32_t)len << CSH);
             }
             done += len;
             m = (m + len) % N;
@@ -258,7 +260,7 @@ int orc_replay_export(const orc_replay* r, int32_t* start, uint8_t* bonds)
             if (!wn) return 4;
             if (cur == site) break;
             if (wn & LBIT) return 4;
-            here = wn >> 5;
+            here = wn >> CSH;
         }
         if (i + (long)off != N) return 4;
         for (uint32_t k = 0; k < off; k++) b[i++] = 0;

@@ -137,7 +137,7 @@ def test_large_box_invariants_and_conservation():
     m.run(3)
     assert m.check() == 0
     w, rec = m.state()
-    counts = np.where(w & 16, 0, w >> 5).astype(np.int64).sum() + rec[:, 1].astype(np.int64).sum()
+    counts = np.where(w & 16, 0, w >> 16).astype(np.int64).sum() + rec[:, 1].astype(np.int64).sum()
     assert counts == 5000 * 4027
 
 
@@ -182,3 +182,22 @@ def test_bad_inputs_fail_cleanly(tmp_path):
     with pytest.raises(elp.ElpError) as e:
         m.load_chains(clash, b2)
     assert e.value.status == elp.ERR_INTEGRITY
+
+
+@pytest.mark.parametrize("L,N,kw", [(16, 50, dict()), (24, 60, dict()), (32, 100, dict()),
+                                     (64, 200, dict(periodic=0, tile=(32, 32, 32))),
+                                     (64, 200, dict(periodic=0, tile=(32, 32, 16))),
+                                     (32, 100, dict(periodic=0, tile=(16, 16, 16))),
+                                     (48, 100, dict(periodic=0, tile=(48, 24, 24)))])
+def test_specialised_kernels_equal_generic(L, N, kw):
+    a = elp.Melt(L=L, N=N, seed=31, kernel=0, **kw)
+    b = elp.Melt(L=L, N=N, seed=31, kernel=1, **kw)
+    a.init_melt()
+    b.init_melt()
+    for _ in range(5):
+        a.run(7)
+        b.run(7)
+        wa, ra = a.state()
+        wb, rb = b.state()
+        assert np.array_equal(wa, wb) and np.array_equal(ra, rb)
+    assert a.accepted() == b.accepted()
