@@ -64,6 +64,7 @@ typedef struct elp_info {
     int32_t periodic, tile[3], ncol;
     int32_t domains;          /* CTAs per step */
     int32_t threads;          /* threads per CTA */
+    int32_t specialised;      /* 1: a shape-specialised kernel runs this melt, 0: generic kernel */
     uint64_t smem_bytes;      /* dynamic shared memory per CTA */
     uint64_t step;            /* absolute steps done */
     uint64_t device_bytes;    /* device memory held by the context */
@@ -133,6 +134,36 @@ elp_status elp_format_tuv(int32_t L, int32_t N, int32_t P, const int32_t* start,
 
 const char* elp_status_string(elp_status s);
 const char* elp_last_error(void);
+
+/* ---- batched engine --------------------------------------------------------
+ * Many independent melts (replicas, seeds, parameter sweeps) of uneven box
+ * size and ring length advanced together on one GPU.  All lattices live in
+ * one packed arena; melts with the same domain geometry share one kernel
+ * launch and a stream, and groups of different shapes run concurrently.
+ * Whole-box melts (L <= 32) run `steps_per_launch` steps per launch on chip;
+ * tiled melts run one step per launch, replayed from a CUDA graph.  A melt
+ * gives the same bits in a batch as alone with the same spec.
+ * The reference has no batched engine; its nearest form is one independent
+ * replica per GPU (gpupol2/gpupol_init.c:8-33, gpupol2/gpupol_cuda.cu:129-146). */
+typedef struct elp_batch elp_batch;
+
+elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs, int32_t device, elp_batch** out);
+int32_t elp_batch_size(const elp_batch* b);
+/* Reference initial melt for every member (step 0). */
+elp_status elp_batch_init_melts(elp_batch* b);
+elp_status elp_batch_load_chains(elp_batch* b, int32_t job, const int32_t* start, const uint8_t* bonds,
+                                 uint64_t step);
+/* Advance every member by nsteps (asynchronous). */
+elp_status elp_batch_run(elp_batch* b, int64_t nsteps);
+/* Same, timed with CUDA events across all group streams; blocks. */
+elp_status elp_batch_run_timed(elp_batch* b, int64_t nsteps, float* ms);
+elp_status elp_batch_sync(elp_batch* b);
+elp_status elp_batch_fetch_chains(elp_batch* b, int32_t job, int32_t* start, uint8_t* bonds);
+elp_status elp_batch_get_state(elp_batch* b, int32_t job, uint32_t* words, uint32_t* records);
+elp_status elp_batch_check(elp_batch* b, int32_t job, int32_t* code);
+elp_status elp_batch_accepted(elp_batch* b, int32_t job, uint64_t* accepted);
+elp_status elp_batch_job_info(const elp_batch* b, int32_t job, elp_info* info);
+void elp_batch_destroy(elp_batch* b);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,353 @@
+// elp_batch.cu -- the batched engine: many independent melts (replicas,
+// seeds, parameter sweeps) of uneven box size and ring length advanced
+// together on one GPU.
+//
+// All lattices and chain records live in one packed ragged arena.  Melts with
+// the same domain geometry form a group (elp_group.h) that one kernel launch
+// serves: whole-box melts (L <= 32) run many steps per launch without leaving
+// shared memory; tiled melts run one step per launch, replayed from a CUDA
+// graph.  Every group has its own stream, so groups of different shapes run
+// concurrently.  A melt gives the same bits in a batch as alone (same kernel,
+// same counters).
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "elp_common.h"
+#include "elp_group.h"
+#include "elp_kernels.h"
+
+namespace {
+struct Member {
+    int group, index;          // group and position inside it
+    elp_geometry g;
+    int N, P;
+    uint32_t seed, salt;
+    uint32_t* lat;
+    uint32_t* rec;
+    unsigned long long* acc;
+    int loaded;
+};
+}  // namespace
+
+struct elp_batch {
+    int device = 0, nsm = 148;
+    std::vector<Member> m;
+    std::vector<elp_group*> groups;
+    std::vector<cudaStream_t> streams;
+    cudaStream_t main = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> done;
+    uint32_t* d_lat = nullptr;
+    uint32_t* d_rec = nullptr;
+    unsigned long long* d_acc = nullptr;   // one per melt
+    uint32_t* d_err = nullptr;             // one per group
+    uint32_t* d_table = nullptr;
+    size_t device_bytes = 0;
+    elp_walk_bufs wb;
+};
+
+extern "C" void elp_batch_destroy(elp_batch* b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    for (cudaStream_t s : b->streams) cudaStreamSynchronize(s);
+    for (elp_group* G : b->groups) {
+        elp_group_free(G);
+        delete G;
+    }
+    elp_walk_bufs_free(&b->wb);
+    for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->done) cudaEventDestroy(e);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->main) cudaStreamDestroy(b->main);
+    cudaFree(b->d_lat); cudaFree(b->d_rec); cudaFree(b->d_acc); cudaFree(b->d_err); cudaFree(b->d_table);
+    delete b;
+}
+
+extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs, int32_t device, elp_batch** out)
+{
+    if (!specs || !out || njobs < 1) return elp_fail(ELP_ERR_ARG, "bad argument");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return elp_fail(ELP_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return elp_fail(ELP_ERR_ARG, "device %d not present", device);
+    ELP_CUDA_TRY(cudaSetDevice(device));
+    elp_batch* b = new (std::nothrow) elp_batch();
+    if (!b) return elp_fail(ELP_ERR_NOMEM, "host allocation failed");
+    b->device = device;
+    if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || b->nsm < 1) b->nsm = 148;
+
+    // resolve every melt; group by geometry, steps per launch and kernel choice
+    std::map<std::tuple<int, int, int, int, int, int, int, int>, int> key2g;
+    std::vector<std::tuple<elp_geometry, int, int>> gdesc;  // geometry, spl, generic
+    size_t lat_words = 0, rec_words = 0;
+    elp_status st = ELP_OK;
+    for (int j = 0; j < njobs; j++) {
+        Member mm;
+        memset(&mm, 0, sizeof(mm));
+        st = elp_resolve_spec(&specs[j], &mm.P, &mm.g);
+        if (st) {
+            elp_batch_destroy(b);
+            return elp_fail(st, "melt %d: %s", j, elp_last_error());
+        }
+        mm.N = specs[j].N;
+        mm.seed = specs[j].seed;
+        mm.salt = specs[j].salt;
+        const int spl = mm.g.periodic ? (specs[j].steps_per_launch > 0 ? specs[j].steps_per_launch : 1) : 1;
+        const int gen = specs[j].kernel == 1;
+        auto key = std::make_tuple(mm.g.periodic, mm.g.L, mm.g.tx, mm.g.ty, mm.g.tz, mm.g.ncol, spl, gen);
+        auto it = key2g.find(key);
+        if (it == key2g.end()) {
+            it = key2g.emplace(key, (int)gdesc.size()).first;
+            gdesc.emplace_back(mm.g, spl, gen);
+        }
+        mm.group = it->second;
+        b->m.push_back(mm);
+        lat_words += ((size_t)mm.g.L * mm.g.L * mm.g.L + 63) / 64 * 64;
+        rec_words += (size_t)mm.P * ELP_REC_WORDS;
+    }
+    // one packed arena for all lattices and records
+    e = cudaMalloc((void**)&b->d_lat, lat_words * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_rec, rec_words * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_acc, (size_t)njobs * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_err, gdesc.size() * sizeof(uint32_t) * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_table, 4096);
+    if (e != cudaSuccess) {
+        elp_batch_destroy(b);
+        return elp_fail(e == cudaErrorMemoryAllocation ? ELP_ERR_NOMEM : ELP_ERR_CUDA, "arena allocation failed: %s",
+                        cudaGetErrorString(e));
+    }
+    b->device_bytes = lat_words * 4 + rec_words * 4 + (size_t)njobs * 8 + gdesc.size() * 16 + 4096;
+    uint8_t tab[4096];
+    elp_build_table(tab);
+    if (cudaMemcpy(b->d_table, tab, 4096, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->d_lat, 0, lat_words * 4) != cudaSuccess ||
+        cudaMemset(b->d_acc, 0, (size_t)njobs * 8) != cudaSuccess ||
+        cudaMemset(b->d_err, 0, gdesc.size() * 16) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev0, cudaEventDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev1, cudaEventDefault) != cudaSuccess) {
+        elp_batch_destroy(b);
+        return elp_fail(ELP_ERR_CUDA, "batch set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    size_t lo = 0, ro = 0;
+    for (size_t g = 0; g < gdesc.size(); g++) {
+        cudaStream_t s;
+        cudaEvent_t ev;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            elp_batch_destroy(b);
+            return elp_fail(ELP_ERR_CUDA, "stream creation failed");
+        }
+        b->streams.push_back(s);
+        b->done.push_back(ev);
+        elp_group* G = new elp_group();
+        b->groups.push_back(G);
+        if (elp_group_init(G, std::get<0>(gdesc[g]), b->nsm, std::get<2>(gdesc[g]), std::get<1>(gdesc[g]), b->d_table,
+                           b->d_err + 4 * g, s) != cudaSuccess) {
+            elp_batch_destroy(b);
+            return elp_fail(ELP_ERR_CUDA, "group set-up failed");
+        }
+    }
+    for (size_t j = 0; j < b->m.size(); j++) {
+        Member& mm = b->m[j];
+        mm.lat = b->d_lat + lo;
+        mm.rec = b->d_rec + ro;
+        mm.acc = b->d_acc + j;
+        lo += ((size_t)mm.g.L * mm.g.L * mm.g.L + 63) / 64 * 64;
+        ro += (size_t)mm.P * ELP_REC_WORDS;
+        elp_group* G = b->groups[(size_t)mm.group];
+        mm.index = (int)G->jobs.size();
+        elp_group_add(G, mm.lat, mm.rec, mm.acc, mm.N, mm.P, mm.seed, mm.salt, 0);
+    }
+    for (elp_group* G : b->groups) {
+        if ((e = elp_group_commit(G)) != cudaSuccess) {
+            elp_batch_destroy(b);
+            return elp_fail(ELP_ERR_CUDA, "group commit failed: %s", cudaGetErrorString(e));
+        }
+    }
+    *out = b;
+    return ELP_OK;
+}
+
+extern "C" int32_t elp_batch_size(const elp_batch* b) { return b ? (int32_t)b->m.size() : 0; }
+
+static elp_status job_ok(const elp_batch* b, int32_t j)
+{
+    if (!b) return elp_fail(ELP_ERR_ARG, "null batch");
+    if (j < 0 || (size_t)j >= b->m.size()) return elp_fail(ELP_ERR_ARG, "melt %d out of range", j);
+    return ELP_OK;
+}
+
+static elp_status errors_of(elp_batch* b, int g)
+{
+    return elp_device_errors(b->d_err + 4 * (size_t)g, b->streams[(size_t)g]);
+}
+
+extern "C" elp_status elp_batch_load_chains(elp_batch* b, int32_t j, const int32_t* start, const uint8_t* bonds,
+                                            uint64_t step)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    if (!start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
+    Member& mm = b->m[(size_t)j];
+    const size_t S = (size_t)mm.g.L * mm.g.L * mm.g.L;
+    std::vector<uint32_t> lat(S), rec((size_t)mm.P * ELP_REC_WORDS);
+    int rc = elp_chains_to_sites(mm.g.L, mm.N, mm.P, start, bonds, lat.data(), rec.data());
+    if (rc == 3) return elp_fail(ELP_ERR_INTEGRITY, "melt %d: two runs share a site (code 3)", j);
+    if (rc) return elp_fail(ELP_ERR_INTEGRITY, "melt %d: invalid ring (code 4)", j);
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    cudaStream_t s = b->streams[(size_t)mm.group];
+    ELP_CUDA_TRY(cudaMemcpyAsync(mm.lat, lat.data(), S * 4, cudaMemcpyHostToDevice, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(mm.rec, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice, s));
+    ELP_CUDA_TRY(elp_group_set_step(b->groups[(size_t)mm.group], mm.index, step));
+    ELP_CUDA_TRY(cudaStreamSynchronize(s));
+    mm.loaded = 1;
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_batch_init_melts(elp_batch* b)
+{
+    if (!b) return elp_fail(ELP_ERR_ARG, "null batch");
+    for (size_t j = 0; j < b->m.size(); j++) {
+        const Member& mm = b->m[j];
+        std::vector<int32_t> start((size_t)mm.P * 3);
+        std::vector<uint8_t> bonds((size_t)mm.P * mm.N);
+        if (elp_initial_chains(mm.g.L, mm.N, mm.P, start.data(), bonds.data()))
+            return elp_fail(ELP_ERR_ARG, "melt %zu: initial grid cannot hold %d rings of %d in L=%d", j, mm.P, mm.N,
+                            mm.g.L);
+        elp_status st = elp_batch_load_chains(b, (int32_t)j, start.data(), bonds.data(), 0);
+        if (st) return st;
+    }
+    return ELP_OK;
+}
+
+static elp_status enqueue(elp_batch* b, int64_t nsteps)
+{
+    for (const Member& mm : b->m)
+        if (!mm.loaded) return elp_fail(ELP_ERR_STATE, "a melt of the batch has no configuration");
+    for (elp_group* G : b->groups) ELP_CUDA_TRY(elp_group_run(G, nsteps));
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_batch_run(elp_batch* b, int64_t nsteps)
+{
+    if (!b) return elp_fail(ELP_ERR_ARG, "null batch");
+    if (nsteps < 0) return elp_fail(ELP_ERR_ARG, "negative step count");
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    return enqueue(b, nsteps);
+}
+
+extern "C" elp_status elp_batch_run_timed(elp_batch* b, int64_t nsteps, float* ms)
+{
+    if (!b || !ms) return elp_fail(ELP_ERR_ARG, "null argument");
+    if (nsteps < 0) return elp_fail(ELP_ERR_ARG, "negative step count");
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    for (cudaStream_t s : b->streams) ELP_CUDA_TRY(cudaStreamSynchronize(s));
+    ELP_CUDA_TRY(cudaEventRecord(b->ev0, b->main));
+    for (cudaStream_t s : b->streams) ELP_CUDA_TRY(cudaStreamWaitEvent(s, b->ev0, 0));
+    elp_status st = enqueue(b, nsteps);
+    if (st) return st;
+    for (size_t g = 0; g < b->streams.size(); g++) {
+        ELP_CUDA_TRY(cudaEventRecord(b->done[g], b->streams[g]));
+        ELP_CUDA_TRY(cudaStreamWaitEvent(b->main, b->done[g], 0));
+    }
+    ELP_CUDA_TRY(cudaEventRecord(b->ev1, b->main));
+    ELP_CUDA_TRY(cudaEventSynchronize(b->ev1));
+    ELP_CUDA_TRY(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    for (size_t g = 0; g < b->groups.size(); g++) {
+        st = errors_of(b, (int)g);
+        if (st) return st;
+    }
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_batch_sync(elp_batch* b)
+{
+    if (!b) return elp_fail(ELP_ERR_ARG, "null batch");
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    for (size_t g = 0; g < b->groups.size(); g++) {
+        elp_status st = errors_of(b, (int)g);
+        if (st) return st;
+    }
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_batch_fetch_chains(elp_batch* b, int32_t j, int32_t* start, uint8_t* bonds)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    if (!start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
+    const Member& mm = b->m[(size_t)j];
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    if ((st = errors_of(b, mm.group))) return st;
+    return elp_fetch_rings(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, start, bonds, b->streams[(size_t)mm.group]);
+}
+
+extern "C" elp_status elp_batch_get_state(elp_batch* b, int32_t j, uint32_t* words, uint32_t* records)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    if (!words || !records) return elp_fail(ELP_ERR_ARG, "null argument");
+    const Member& mm = b->m[(size_t)j];
+    cudaStream_t s = b->streams[(size_t)mm.group];
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    ELP_CUDA_TRY(cudaMemcpyAsync(words, mm.lat, (size_t)mm.g.L * mm.g.L * mm.g.L * 4, cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(records, mm.rec, (size_t)mm.P * ELP_REC_WORDS * 4, cudaMemcpyDeviceToHost, s));
+    return errors_of(b, mm.group);
+}
+
+extern "C" elp_status elp_batch_check(elp_batch* b, int32_t j, int32_t* code)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    if (!code) return elp_fail(ELP_ERR_ARG, "null argument");
+    const Member& mm = b->m[(size_t)j];
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    if ((st = errors_of(b, mm.group))) return st;
+    return elp_check_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, code, b->streams[(size_t)mm.group]);
+}
+
+extern "C" elp_status elp_batch_accepted(elp_batch* b, int32_t j, uint64_t* acc)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    if (!acc) return elp_fail(ELP_ERR_ARG, "null argument");
+    const Member& mm = b->m[(size_t)j];
+    cudaStream_t s = b->streams[(size_t)mm.group];
+    unsigned long long v = 0;
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    ELP_CUDA_TRY(cudaMemcpyAsync(&v, mm.acc, 8, cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaStreamSynchronize(s));
+    *acc = v;
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info* info)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    if (!info) return elp_fail(ELP_ERR_ARG, "null argument");
+    const Member& mm = b->m[(size_t)j];
+    const elp_group* G = b->groups[(size_t)mm.group];
+    memset(info, 0, sizeof(*info));
+    info->L = mm.g.L; info->N = mm.N; info->P = mm.P;
+    info->periodic = mm.g.periodic;
+    info->tile[0] = mm.g.tx; info->tile[1] = mm.g.ty; info->tile[2] = mm.g.tz;
+    info->ncol = mm.g.ncol;
+    info->domains = mm.g.periodic ? 1 : (mm.g.L / mm.g.tx) * (mm.g.L / mm.g.ty) * (mm.g.L / mm.g.tz);
+    info->threads = (G->lay.groups + 31) / 32 * 32;
+    info->specialised = G->specialised;
+    info->smem_bytes = G->lay.bytes;
+    info->step = elp_group_step(G, mm.index);
+    info->device_bytes = b->device_bytes + b->wb.bytes;
+    return ELP_OK;
+}

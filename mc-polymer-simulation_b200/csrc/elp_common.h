@@ -1,0 +1,51 @@
+// elp_common.h -- pieces shared by the single-melt and batch C ABIs: error
+// reporting, geometry choice, device-side ring reconstruction and checks,
+// TUV text parsing.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/elp.h"
+#include "elp_internal.h"
+
+// Record a message for elp_last_error() and return `s`.
+elp_status elp_fail(elp_status s, const char* fmt, ...);
+
+#define ELP_CUDA_TRY(call)                                                                           \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return elp_fail(e_ == cudaErrorMemoryAllocation ? ELP_ERR_NOMEM : ELP_ERR_CUDA,          \
+                            "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);    \
+    } while (0)
+
+// Rings and geometry of a job spec; returns ELP_OK or ELP_ERR_ARG.
+elp_status elp_resolve_spec(const elp_job_spec* spec, int* P, elp_geometry* g);
+
+// Device error flags written by kernels instead of trapping.
+elp_status elp_device_errors(const uint32_t* d_flags, cudaStream_t s);
+
+// Scratch buffers for walking rings on the device.
+struct elp_walk_bufs {
+    int32_t* d_start = nullptr;
+    uint8_t* d_bonds = nullptr;
+    int32_t* d_status = nullptr;
+    uint32_t* d_visit = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0;
+    size_t bytes = 0;
+};
+void elp_walk_bufs_free(elp_walk_bufs* b);
+
+// Rebuild rings (start[3P], bonds[P*N]) of one melt into host buffers.
+elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+                           int32_t* start, uint8_t* bonds, cudaStream_t s);
+// Integrity check of one melt (code 0, 3 or 4 as CheckIntegrity).
+elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+                          int32_t* code, cudaStream_t s);
+
+// Parse TUV text for a melt of box L, P rings of N.  Returns ELP_OK or
+// ELP_ERR_FORMAT (message set).
+elp_status elp_parse_tuv(const char* text, const char* name, int L, int N, int P, int32_t* start, uint8_t* bonds);
+elp_status elp_read_file(const char* path, char** text, size_t* len);

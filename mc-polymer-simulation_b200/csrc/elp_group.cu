@@ -1,0 +1,212 @@
+// elp_group.cu -- launching the sweep for a group of melts (see elp_group.h).
+#include <string.h>
+
+#include "elp_group.h"
+
+namespace {
+__global__ void ctr_add_kernel(uint32_t* c, uint32_t v) { *c += v; }
+
+int domains_of(const elp_geometry& g)
+{
+    return g.periodic ? 1 : (g.L / g.tx) * (g.L / g.ty) * (g.L / g.tz);
+}
+
+Sweep2Launch make_launch(const elp_group* G, int nsteps, uint32_t step_base, int check_only)
+{
+    Sweep2Launch l;
+    memset(&l, 0, sizeof(l));
+    l.geom = G->g;
+    l.sx = G->lay.sx;
+    l.sxy = G->lay.sxy;
+    l.nsm = G->nsm;
+    l.check_only = check_only;
+    double sites = (double)G->g.tx * G->g.ty * G->g.tz, box = (double)G->g.L * G->g.L * G->g.L;
+    for (const BatchJob& j : G->jobs) {
+        double m = j.nchains * sites / box;
+        if (m > l.max_runs_per_domain) l.max_runs_per_domain = m;
+    }
+    l.args.jobs = G->d_jobs;
+    l.args.items = G->d_items;
+    l.args.nitems = G->nitems;
+    l.args.nsteps = nsteps;
+    l.args.step_base = step_base;
+    l.args.step_dev = G->d_ctr;
+    l.args.table = G->d_table;
+    l.args.error = G->d_error;
+    return l;
+}
+
+// Generic kernel: one launch per melt, absolute step known on the host.
+cudaError_t launch_generic(elp_group* G, int nsteps)
+{
+    for (size_t j = 0; j < G->jobs.size(); j++) {
+        const BatchJob& J = G->jobs[j];
+        SweepArgs a;
+        memset(&a, 0, sizeof(a));
+        a.lat = J.lat;
+        a.rec = J.rec;
+        a.table = G->d_table;
+        a.accepted = J.acc;
+        a.error = G->d_error;
+        a.nchains = J.nchains;
+        a.L = G->g.L;
+        a.periodic = G->g.periodic;
+        a.tx = G->g.tx; a.ty = G->g.ty; a.tz = G->g.tz;
+        a.ncol = G->g.ncol;
+        a.sx = G->lay.sx; a.sxy = G->lay.sxy; a.ox = G->lay.ox;
+        a.words = G->lay.words;
+        a.groups = G->lay.groups;
+        a.seed = J.seed;
+        a.salt = J.salt;
+        a.step0 = (uint32_t)(J.step0 + (uint32_t)G->steps_done);
+        a.nsteps = nsteps;
+        int threads = (G->lay.groups + 31) / 32 * 32;
+        cudaError_t e = elp_launch_sweep(&a, domains_of(G->g), threads < 32 ? 32 : threads, G->lay.bytes, G->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_once(elp_group* G, int nsteps, uint32_t step_base)
+{
+    if (!G->specialised) return launch_generic(G, nsteps);
+    Sweep2Launch l = make_launch(G, nsteps, step_base, 0);
+    return elp_launch_sweep2(&l, G->stream);
+}
+}  // namespace
+
+cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int generic, int spl,
+                           const uint32_t* d_table, uint32_t* d_error, cudaStream_t stream)
+{
+    G->g = geom;
+    elp_layout(&geom, &G->lay);
+    G->nsm = nsm;
+    G->generic = generic;
+    G->spl = spl > 0 ? spl : 1;
+    G->use_graph = !geom.periodic;
+    G->graph_steps = 50;
+    G->stream = stream;
+    G->d_table = d_table;
+    G->d_error = d_error;
+    cudaError_t e = cudaMalloc((void**)&G->d_ctr, sizeof(uint32_t));
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(G->d_ctr, 0, sizeof(uint32_t), stream);
+}
+
+void elp_group_add(elp_group* G, uint32_t* lat, uint32_t* rec, unsigned long long* acc, int N, int nchains,
+                   uint32_t seed, uint32_t salt, uint64_t step)
+{
+    BatchJob j;
+    memset(&j, 0, sizeof(j));
+    j.lat = lat;
+    j.rec = rec;
+    j.acc = acc;
+    j.L = G->g.L;
+    j.nchains = nchains;
+    j.ntx = G->g.periodic ? 1 : G->g.L / G->g.tx;
+    j.nty = G->g.periodic ? 1 : G->g.L / G->g.ty;
+    j.ntz = G->g.periodic ? 1 : G->g.L / G->g.tz;
+    j.seed = seed;
+    j.salt = salt;
+    j.step0 = (uint32_t)(step - G->steps_done);
+    G->jobs.push_back(j);
+    G->N.push_back(N);
+}
+
+cudaError_t elp_group_commit(elp_group* G)
+{
+    const int nd = domains_of(G->g);
+    const size_t nj = G->jobs.size();
+    cudaError_t e;
+    if (G->d_jobs) cudaFree(G->d_jobs);
+    if (G->d_items) cudaFree(G->d_items);
+    G->d_jobs = nullptr;
+    G->d_items = nullptr;
+    if ((e = cudaMalloc((void**)&G->d_jobs, nj * sizeof(BatchJob))) != cudaSuccess) return e;
+    if ((e = cudaMalloc((void**)&G->d_items, nj * nd * sizeof(uint2))) != cudaSuccess) return e;
+    std::vector<uint2> items(nj * nd);
+    // domain-major order: the first wave of a persistent grid spreads over melts
+    for (int d = 0; d < nd; d++)
+        for (size_t j = 0; j < nj; j++) items[(size_t)d * nj + j] = make_uint2((uint32_t)j, (uint32_t)d);
+    G->nitems = (int)items.size();
+    if ((e = cudaMemcpyAsync(G->d_jobs, G->jobs.data(), nj * sizeof(BatchJob), cudaMemcpyHostToDevice, G->stream)))
+        return e;
+    if ((e = cudaMemcpyAsync(G->d_items, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                             G->stream)))
+        return e;
+    Sweep2Launch l = make_launch(G, G->g.periodic ? G->spl : 1, 0, 1);
+    G->specialised = !G->generic && elp_launch_sweep2(&l, G->stream) == cudaSuccess;
+    if (G->graph) {
+        cudaGraphExecDestroy(G->graph);
+        G->graph = nullptr;
+    }
+    return cudaStreamSynchronize(G->stream);
+}
+
+cudaError_t elp_group_set_step(elp_group* G, int j, uint64_t step)
+{
+    G->jobs[(size_t)j].step0 = (uint32_t)(step - G->steps_done);
+    return cudaMemcpyAsync(G->d_jobs + j, &G->jobs[(size_t)j], sizeof(BatchJob), cudaMemcpyHostToDevice, G->stream);
+}
+
+uint64_t elp_group_step(const elp_group* G, int j)
+{
+    return (uint64_t)G->jobs[(size_t)j].step0 + G->steps_done;
+}
+
+cudaError_t elp_group_run(elp_group* G, int64_t nsteps)
+{
+    cudaError_t e;
+    if (G->g.periodic) {
+        while (nsteps > 0) {
+            int k = (int)(nsteps < G->spl ? nsteps : G->spl);
+            if ((e = launch_once(G, k, (uint32_t)(G->steps_done - G->ctr_mirror))) != cudaSuccess) return e;
+            G->steps_done += (uint64_t)k;
+            nsteps -= k;
+        }
+        return cudaSuccess;
+    }
+    if (G->specialised && G->use_graph && nsteps >= G->graph_steps) {
+        const uint32_t base = (uint32_t)(G->steps_done - G->ctr_mirror);
+        if (!G->graph || G->graph_base != base) {
+            if (G->graph) cudaGraphExecDestroy(G->graph);
+            G->graph = nullptr;
+            cudaGraph_t gr;
+            if ((e = cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+            for (int i = 0; i < G->graph_steps; i++) {
+                Sweep2Launch l = make_launch(G, 1, base + (uint32_t)i, 0);
+                elp_launch_sweep2(&l, G->stream);
+            }
+            ctr_add_kernel<<<1, 1, 0, G->stream>>>(G->d_ctr, (uint32_t)G->graph_steps);
+            if ((e = cudaStreamEndCapture(G->stream, &gr)) != cudaSuccess) return e;
+            e = cudaGraphInstantiate(&G->graph, gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) return e;
+            G->graph_base = base;
+        }
+        while (nsteps >= G->graph_steps) {
+            if ((e = cudaGraphLaunch(G->graph, G->stream)) != cudaSuccess) return e;
+            G->steps_done += (uint64_t)G->graph_steps;
+            G->ctr_mirror += (uint32_t)G->graph_steps;
+            nsteps -= G->graph_steps;
+        }
+    }
+    while (nsteps > 0) {
+        if ((e = launch_once(G, 1, (uint32_t)(G->steps_done - G->ctr_mirror))) != cudaSuccess) return e;
+        G->steps_done += 1;
+        nsteps -= 1;
+    }
+    return cudaSuccess;
+}
+
+void elp_group_free(elp_group* G)
+{
+    if (G->graph) cudaGraphExecDestroy(G->graph);
+    cudaFree(G->d_jobs);
+    cudaFree(G->d_items);
+    cudaFree(G->d_ctr);
+    G->graph = nullptr;
+    G->d_jobs = nullptr;
+    G->d_items = nullptr;
+    G->d_ctr = nullptr;
+}

@@ -28,9 +28,41 @@ struct WalkArgs {
     unsigned long long* counters;  // [5]: runs walked, runs found, monomers found, bad sites, shared sites
 };
 
+// One melt of a batch as the specialised kernel sees it.
+struct BatchJob {
+    uint32_t* lat;                 // its L^3 site words
+    uint32_t* rec;                 // its chain records
+    unsigned long long* acc;       // its accepted-move counter (or null)
+    int L, nchains;
+    int ntx, nty, ntz;             // domains per axis
+    uint32_t seed, salt;
+    uint32_t step0;                // absolute step at step_base == 0
+};
+
+struct BatchLaunch {
+    const BatchJob* jobs;          // device job table
+    const uint2* items;            // device work items {job, domain}
+    int nitems;
+    int nsteps;                    // steps per launch (whole-box domains only; else 1)
+    uint32_t step_base;            // added to every job's step0 ...
+    const uint32_t* step_dev;      // ... and, if set, this device counter (graph replays)
+    const uint32_t* table;         // 4096-byte transition table
+    uint32_t* error;               // device error flags
+};
+
+#include "elp_internal.h"
+struct Sweep2Launch {
+    elp_geometry geom;
+    int sx, sxy;                   // shared-memory strides of the layout
+    int nsm;                       // SMs for the persistent grid
+    int check_only;                // only report whether a kernel fits
+    double max_runs_per_domain;    // expected monomer-0 runs in one domain
+    BatchLaunch args;
+};
+
 extern "C" {
 cudaError_t elp_launch_sweep(const SweepArgs* a, int ndomains, int threads, size_t smem, cudaStream_t s);
-cudaError_t elp_launch_sweep2(const SweepArgs* a, int nsm, cudaStream_t s);
+cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s);
 cudaError_t elp_launch_walk(const WalkArgs* a, cudaStream_t s);
 cudaError_t elp_launch_scan(const WalkArgs* a, cudaStream_t s);
 }

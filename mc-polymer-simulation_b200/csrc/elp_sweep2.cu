@@ -14,6 +14,7 @@
 //   * tiles are fetched with cp.async (4-byte granules: the origin shift
 //     makes rows unaligned) and the grid is persistent over the tiles.
 #include <cuda_runtime.h>
+#include <math.h>
 
 #include "elp_device.cuh"
 #include "elp_kernels.h"
@@ -41,14 +42,19 @@ struct Shape {
 
 constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
 
+extern __shared__ __align__(16) uint32_t g_smem[];
+
 // Four anchors of one thread, one substep.  Returns accepted moves.
-template <bool PER, int NC>
-__device__ __forceinline__ int substep4(uint32_t* S, const uint8_t* tab, const int* offs, uint32_t* slot_off,
-                                        int* slot_site, const int (&base)[4], const int (&rot)[4],
+// Shared-memory word indices: lattice at 0, transition table (bytes) at
+// TABW words, neighbour offsets at OFFW words.
+template <bool PER, int NC, int TABW, int OFFW>
+__device__ __forceinline__ int substep4(uint32_t* slot_off, int* slot_site, const int (&base)[4], const int (&rot)[4],
                                         const int (&clsyz)[4], const int (&xj)[4], int c, uint32_t w, int L)
 {
-    int p[4];
-    const int* off[4];
+    uint32_t* S = g_smem;
+    const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
+    const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
+    int p[4], ob[4];
     uint32_t wP[4], rb[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -60,19 +66,22 @@ __device__ __forceinline__ int substep4(uint32_t* S, const uint8_t* tab, const i
             int x = xr + xj[q];
             cls += x == 0 ? 0 : (x == L - 1 ? 2 : 1);
         }
-        off[q] = offs + 16 * cls;
+        ob[q] = 16 * cls;
         wP[q] = S[p[q]];
         rb[q] = (w >> (8 * q)) & 0xffu;
     }
-    // stage B: the next run (slot 1)
+    // stage B: the next run (slot 1).  Loaded unconditionally: the index is
+    // inside the anchor's radius-1 ball, which no other anchor of this
+    // substep touches.
     int pB[4];
     uint32_t wB[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        pB[q] = p[q] + off[q][wP[q] & 15];
-        wB[q] = ((rb[q] & 1) && wP[q]) ? S[pB[q]] : 0u;
+        pB[q] = p[q] + offs[ob[q] + (wP[q] & 15)];
+        wB[q] = S[pB[q]];
     }
-    // stage C: source bonds (b_{m-1}, b_m) and the table option
+    // stage C: source bonds (b_{m-1}, b_m) and the table option.  Slot 0 needs
+    // a run of at least two, slot 1 a next run inside the domain.
     uint32_t e[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -80,17 +89,18 @@ __device__ __forceinline__ int substep4(uint32_t* S, const uint8_t* tab, const i
         const bool live = wP[q] != 0 && (s ? wB[q] != ELP_WALL : wP[q] >= 2u * ELP_CUNIT);
         const uint32_t src2 = s ? ((wB[q] >= 2u * ELP_CUNIT) ? 0u : (wB[q] & 15)) : bo;
         const uint32_t idx = ((s ? bo : 0u) << 8) | (src2 << 4) | ((rb[q] >> 1) & 15);
-        e[q] = live ? (uint32_t)tab[idx] : 0u;
+        e[q] = tab[live ? idx : 0xFF0u];   // row (0xf, 0xf) holds only null moves
     }
-    // stage D: target site P + dst1
+    // stage D: target site P + dst1 (again inside the ball)
     int pY[4];
     uint32_t wY[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        pY[q] = p[q] + off[q][e[q] & 15];
-        wY[q] = e[q] ? S[pY[q]] : 0u;
+        pY[q] = p[q] + offs[ob[q] + (e[q] & 15)];
+        wY[q] = S[pY[q]];
     }
-    // stage E: accept, label bookkeeping, write
+    // stage E: accept, label bookkeeping, write.  Store order B, Y, P: when
+    // dst1 == 0 the target is P itself and P's store must come last.
     int acc = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -126,23 +136,24 @@ __device__ __forceinline__ int substep4(uint32_t* S, const uint8_t* tab, const i
             slot_off[slot] = noff;
             slot_site[slot] = nl == 0 ? p[q] : (nl == 1 ? pB[q] : pY[q]);
         }
-        if (ok) S[p[q]] = nP;
         if (ok && s) S[pB[q]] = nB;
         if (ok && d1) S[pY[q]] = nY;
+        if (ok) S[p[q]] = nP;
         acc += ok ? 1 : 0;
     }
     return acc;
 }
 
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
+__global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 {
     using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP>;
     static_assert(SH::G <= THREADS, "threads");
     static_assert(CAP <= 2048, "slot numbers are 11 bits");
-    extern __shared__ __align__(16) uint32_t smem[];
-    uint32_t* S = smem;
-    uint8_t* tab = reinterpret_cast<uint8_t*>(smem + SH::WORDS);
+    static_assert((2 * NC) % 4 == 0, "substeps come in groups of four");
+    constexpr int TABW = SH::WORDS, OFFW = SH::WORDS + 1024;
+    uint32_t* S = g_smem;
+    uint8_t* tab = reinterpret_cast<uint8_t*>(g_smem + TABW);
     int* offs = reinterpret_cast<int*>(tab + 4096);
     uint32_t* col = reinterpret_cast<uint32_t*>(offs + 27 * 16);
     uint32_t* slot_chain = col + 64;
@@ -150,8 +161,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
     int* slot_site = reinterpret_cast<int*>(slot_off + CAP);
     uint32_t* nslots = reinterpret_cast<uint32_t*>(slot_site + CAP);
     const int tid = threadIdx.x;
-    const int L = a.L;
-    const uint2 key = make_uint2(a.seed, a.salt);
+    const int LP = TX;  // box edge of whole-box (periodic) domains
 
     for (int i = tid; i < 1024; i += THREADS) reinterpret_cast<uint32_t*>(tab)[i] = a.table[i];
     for (int i = tid; i < 27 * 16; i += THREADS) {
@@ -159,12 +169,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
         int dt = elp_bt(b), du = elp_bu(b), dv = elp_bv(b);
         if (PER) {
             int cx = cls % 3, cy = (cls / 3) % 3, cz = cls / 9;
-            if (cx == 0 && dt < 0) dt = L - 1;
-            if (cx == 2 && dt > 0) dt = -(L - 1);
-            if (cy == 0 && du < 0) du = L - 1;
-            if (cy == 2 && du > 0) du = -(L - 1);
-            if (cz == 0 && dv < 0) dv = L - 1;
-            if (cz == 2 && dv > 0) dv = -(L - 1);
+            if (cx == 0 && dt < 0) dt = LP - 1;
+            if (cx == 2 && dt > 0) dt = -(LP - 1);
+            if (cy == 0 && du < 0) du = LP - 1;
+            if (cy == 2 && du > 0) du = -(LP - 1);
+            if (cz == 0 && dv < 0) dv = LP - 1;
+            if (cz == 2 && dv > 0) dv = -(LP - 1);
         }
         offs[i] = dt + SX * du + SXY * dv;
     }
@@ -180,69 +190,93 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
         int m = (2 * y + 3 * z) % NC;
         rot[q] = m ? NC - m : 0;
         base[q] = SH::OX + SX * y + SXY * z + NC * j;
-        int cy = y == 0 ? 0 : (y == L - 1 ? 2 : 1);
-        int cz = z == 0 ? 0 : (z == L - 1 ? 2 : 1);
+        int cy = y == 0 ? 0 : (y == LP - 1 ? 2 : 1);
+        int cz = z == 0 ? 0 : (z == LP - 1 ? 2 : 1);
         clsyz[q] = PER ? (3 * cy + 9 * cz) : 13;
         xj[q] = NC * j;
     }
     const bool active = tid < SH::G;
+    const uint32_t step_dev = a.step_dev ? *a.step_dev : 0u;
 
-    Dom D;
-    D.S = S; D.tab = tab; D.rec = a.rec;
-    D.ox = SH::OX; D.sx = SX; D.sxy = SXY; D.L = L;
-    D.x0 = 0; D.y0 = 0; D.z0 = 0;
-
-    const int ntx = L / TX, nty = L / TY, ntz = L / TZ;
-    const int ntiles = PER ? 1 : ntx * nty * ntz;
-    int accepted = 0;
-
-    for (int st = 0; st < a.nsteps; st++) {
-        const uint32_t t = (uint32_t)(a.step0 + st);
-        int sh0 = 0, sh1 = 0, sh2 = 0;
-        if (!PER) {
-            uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
-            sh0 = (int)bounded(sh.x, TX); sh1 = (int)bounded(sh.y, TY); sh2 = (int)bounded(sh.z, TZ);
-        }
+    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
+        const uint2 item = a.items[it];
+        const BatchJob& J = a.jobs[item.x];
+        const int d = (int)item.y;
+        const int L = PER ? LP : J.L;
+        uint32_t* lat = J.lat;
+        uint32_t* rec = J.rec;
+        const int nchains = J.nchains;
+        const uint2 key = make_uint2(J.seed, J.salt);
+        const int ntx = J.ntx, nty = J.nty;
+        Dom D;
+        D.S = S; D.tab = tab; D.rec = rec;
+        D.ox = SH::OX; D.sx = SX; D.sxy = SXY; D.L = L;
+        D.x0 = 0; D.y0 = 0; D.z0 = 0;
+        int accepted = 0;
         bool overflow = false;
-        for (int d = blockIdx.x; d < ntiles; d += gridDim.x) {
+
+        for (int st = 0; st < a.nsteps && !overflow; st++) {
+            const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)st;
             if (!PER) {
-                D.x0 = sh0 + (d % ntx) * TX;
-                D.y0 = sh1 + ((d / ntx) % nty) * TY;
-                D.z0 = sh2 + (d / ntx / nty) * TZ;
+                const uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
+                D.x0 = (int)bounded(sh.x, TX) + (d % ntx) * TX;
+                D.y0 = (int)bounded(sh.y, TY) + ((d / ntx) % nty) * TY;
+                D.z0 = (int)bounded(sh.z, TZ) + (d / ntx / nty) * TZ;
             }
-            if (!PER || st == 0) {
-                __syncthreads();  // the previous tile's stores have read shared memory
+            if (st == 0) {
+                __syncthreads();  // the previous item's stores have read shared memory
                 if (tid == 0) *nslots = 0;
                 for (int i = tid; i < SH::SITES; i += THREADS) {
-                    int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
+                    const int x = i % TX, r = i / TX, y = r % TY, z = r / TY;
                     int gx = D.x0 + x; gx -= gx >= L ? L : 0;
                     int gy = D.y0 + y; gy -= gy >= L ? L : 0;
                     int gz = D.z0 + z; gz -= gz >= L ? L : 0;
-                    cp_async4(S + SH::OX + x + SX * y + SXY * z,
-                              a.lat + (size_t)gx + (size_t)L * ((size_t)gy + (size_t)L * gz));
+                    cp_async4(S + SH::OX + x + SX * y + SXY * z, lat + (uint32_t)(gx + L * (gy + L * gz)));
                 }
                 cp_async_wait_all();
                 __syncthreads();
-                // monomer-0 runs: global chain id -> shared slot, run length inline
-                for (int i = tid; i < SH::SITES; i += THREADS) {
-                    int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
-                    int idx = SH::OX + x + SX * y + SXY * z;
-                    uint32_t wv = S[idx];
-                    if (wv & ELP_LBIT) {
-                        uint32_t slot = atomicAdd(nslots, 1u);
-                        uint32_t chain = wv >> 5;
-                        if (slot < (uint32_t)CAP) {
-                            uint4 r = *reinterpret_cast<const uint4*>(a.rec + ELP_REC_WORDS * (size_t)chain);
-                            slot_chain[slot] = chain;
-                            slot_off[slot] = r.z;
-                            slot_site[slot] = idx;
-                            S[idx] = (wv & 15) | ELP_LBIT | (slot << 5) | (r.y << ELP_CSHIFT);
+                // monomer-0 runs: global chain id -> shared slot, run length inline.
+                // Few rings: find them through the chain records; many: scan the tile.
+                if (nchains * 4 <= SH::SITES) {
+                    for (int ch = tid; ch < nchains; ch += THREADS) {
+                        const uint4 r = *reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)ch);
+                        const int gx = (int)(r.x % (uint32_t)L), gy = (int)((r.x / (uint32_t)L) % (uint32_t)L),
+                                  gz = (int)(r.x / ((uint32_t)L * L));
+                        int x = gx - D.x0; x += x < 0 ? L : 0;
+                        int y = gy - D.y0; y += y < 0 ? L : 0;
+                        int z = gz - D.z0; z += z < 0 ? L : 0;
+                        if (x < TX && y < TY && z < TZ) {
+                            const uint32_t slot = atomicAdd(nslots, 1u);
+                            if (slot < (uint32_t)CAP) {
+                                const int idx = SH::OX + x + SX * y + SXY * z;
+                                slot_chain[slot] = (uint32_t)ch;
+                                slot_off[slot] = r.z;
+                                slot_site[slot] = idx;
+                                S[idx] = (S[idx] & 15) | ELP_LBIT | (slot << 5) | (r.y << ELP_CSHIFT);
+                            }
+                        }
+                    }
+                } else {
+                    for (int i = tid; i < SH::SITES; i += THREADS) {
+                        const int x = i % TX, r = i / TX, y = r % TY, z = r / TY;
+                        const int idx = SH::OX + x + SX * y + SXY * z;
+                        const uint32_t wv = S[idx];
+                        if (wv & ELP_LBIT) {
+                            const uint32_t slot = atomicAdd(nslots, 1u);
+                            const uint32_t chain = wv >> 5;
+                            if (slot < (uint32_t)CAP) {
+                                const uint4 rr = *reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)chain);
+                                slot_chain[slot] = chain;
+                                slot_off[slot] = rr.z;
+                                slot_site[slot] = idx;
+                                S[idx] = (wv & 15) | ELP_LBIT | (slot << 5) | (rr.y << ELP_CSHIFT);
+                            }
                         }
                     }
                 }
             }
             if (tid < (2 * NC + 3) / 4) {
-                uint4 cw = philox(make_uint4(t, (uint32_t)d, (uint32_t)tid | ELP_STREAM_COLOUR, 0), key);
+                const uint4 cw = philox(make_uint4(t, (uint32_t)d, (uint32_t)tid | ELP_STREAM_COLOUR, 0), key);
                 col[4 * tid + 0] = bounded(cw.x, NC);
                 col[4 * tid + 1] = bounded(cw.y, NC);
                 col[4 * tid + 2] = bounded(cw.z, NC);
@@ -250,49 +284,49 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
             }
             __syncthreads();
             if (*nslots > (uint32_t)CAP) {
-                // more monomer-0 runs than slots: leave this tile untouched, report
+                // more monomer-0 runs than slots: leave this domain untouched, report
                 if (tid == 0) atomicOr(a.error, 1u);
                 overflow = true;
-                continue;
+                break;
             }
-
-            uint4 rw = make_uint4(0, 0, 0, 0);
 #pragma unroll 1
-            for (int k = 0; k < 2 * NC; k++) {
-                if (active) {
-                    if ((k & 3) == 0) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
-                    accepted += substep4<PER, NC>(S, tab, offs, slot_off, slot_site, base, rot, clsyz, xj, (int)col[k],
-                                                  word_of(rw, k & 3), L);
-                }
-                __syncthreads();
-            }
-
-            if (!PER || st == a.nsteps - 1) {
-                const uint32_t ns = *nslots;
-                for (uint32_t sl = tid; sl < ns; sl += THREADS) {
-                    int idx = slot_site[sl];
-                    uint32_t wv = S[idx];
-                    uint32_t chain = slot_chain[sl];
-                    *reinterpret_cast<uint4*>(a.rec + ELP_REC_WORDS * (size_t)chain) =
-                        make_uint4(global_site(D, idx), wv >> ELP_CSHIFT, slot_off[sl], 0u);
-                    S[idx] = (wv & 15) | ELP_LBIT | (chain << 5);
-                }
-                __syncthreads();
-                for (int i = tid; i < SH::SITES; i += THREADS) {
-                    int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
-                    int gx = D.x0 + x; gx -= gx >= L ? L : 0;
-                    int gy = D.y0 + y; gy -= gy >= L ? L : 0;
-                    int gz = D.z0 + z; gz -= gz >= L ? L : 0;
-                    a.lat[(size_t)gx + (size_t)L * ((size_t)gy + (size_t)L * gz)] = S[SH::OX + x + SX * y + SXY * z];
+            for (int k = 0; k < 2 * NC; k += 4) {
+                uint4 rw = make_uint4(0, 0, 0, 0);
+                if (active) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                const uint32_t rws[4] = {rw.x, rw.y, rw.z, rw.w};
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    if (active)
+                        accepted += substep4<PER, NC, TABW, OFFW>(slot_off, slot_site, base, rot, clsyz, xj,
+                                                                  (int)col[k + kk], rws[kk], LP);
+                    __syncthreads();
                 }
             }
         }
-        if (PER && overflow) break;  // block-uniform: every thread read the same count
-    }
-    if (a.accepted) {
-        unsigned long long v = (unsigned long long)accepted;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((tid & 31) == 0 && v) atomicAdd(a.accepted, v);
+        if (!overflow) {
+            const uint32_t ns = *nslots;
+            for (uint32_t sl = tid; sl < ns; sl += THREADS) {
+                const int idx = slot_site[sl];
+                const uint32_t wv = S[idx];
+                const uint32_t chain = slot_chain[sl];
+                *reinterpret_cast<uint4*>(rec + ELP_REC_WORDS * (size_t)chain) =
+                    make_uint4(global_site(D, idx), wv >> ELP_CSHIFT, slot_off[sl], 0u);
+                S[idx] = (wv & 15) | ELP_LBIT | (chain << 5);
+            }
+            __syncthreads();
+            for (int i = tid; i < SH::SITES; i += THREADS) {
+                const int x = i % TX, r = i / TX, y = r % TY, z = r / TY;
+                int gx = D.x0 + x; gx -= gx >= L ? L : 0;
+                int gy = D.y0 + y; gy -= gy >= L ? L : 0;
+                int gz = D.z0 + z; gz -= gz >= L ? L : 0;
+                lat[(uint32_t)(gx + L * (gy + L * gz))] = S[SH::OX + x + SX * y + SXY * z];
+            }
+        }
+        if (J.acc) {
+            unsigned long long v = (unsigned long long)accepted;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((tid & 31) == 0 && v) atomicAdd(J.acc, v);
+        }
     }
 }
 
@@ -300,36 +334,35 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(SweepArgs a)
 
 // ---- dispatch ----------------------------------------------------------------
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int THREADS, int MINB>
-static cudaError_t launch2(const SweepArgs* a, int nsm, cudaStream_t s)
+static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 {
     using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP>;
-    // expected monomer-0 runs per tile must stay well inside the slot table
-    double per_tile = (double)a->nchains * SH::SITES / ((double)a->L * a->L * a->L);
-    if (PER ? a->nchains > CAP : per_tile * 4.0 > CAP) return cudaErrorNotSupported;
     auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, THREADS, MINB>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
-        if (e != cudaSuccess) return e;
-        attr = true;
+    if (l->check_only) {
+        // expected monomer-0 runs per domain must stay far inside the slot table
+        const double m = l->max_runs_per_domain;
+        if (!(PER ? m <= CAP : m + 8.0 * sqrt(m) + 16.0 <= CAP)) return cudaErrorNotSupported;
+        // set the shared-memory limit here, outside any stream capture
+        return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
     }
-    int ntiles = PER ? 1 : (a->L / TX) * (a->L / TY) * (a->L / TZ);
-    int grid = ntiles;
-    if (!PER && grid > nsm * MINB) grid = nsm * MINB;
-    k<<<grid, THREADS, SH::BYTES, s>>>(*a);
+    int grid = l->args.nitems;
+    if (grid > l->nsm * MINB) grid = l->nsm * MINB;
+    if (grid < 1) return cudaSuccess;
+    k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
     return cudaGetLastError();
 }
 
-// Returns cudaErrorNotSupported when no specialised kernel fits the job (the
-// caller then uses the generic kernel).
-extern "C" cudaError_t elp_launch_sweep2(const SweepArgs* a, int nsm, cudaStream_t s)
+// Launch (or, with check_only, test) the specialised kernel for a shape.
+// Returns cudaErrorNotSupported when none fits (the caller then uses the
+// generic kernel).
+extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
 {
-    if (a->nsteps > 1 && !a->periodic) return cudaErrorNotSupported;
-    if (!a->error) return cudaErrorNotSupported;
+    const elp_geometry& g = l->geom;
+    if (l->args.nsteps > 1 && !g.periodic) return cudaErrorNotSupported;
 #define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_)                                            \
-    if (a->tx == X_ && a->ty == Y_ && a->tz == Z_ && a->periodic == PER_ && a->ncol == NC_ && a->sx == SX_ &&   \
-        a->sxy == SXY_)                                                                                        \
-        return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_>(a, nsm, s);
+    if (g.tx == X_ && g.ty == Y_ && g.tz == Z_ && g.periodic == PER_ && g.ncol == NC_ && l->sx == SX_ &&       \
+        l->sxy == SXY_)                                                                                        \
+        return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_>(l, s);
     SHAPE(32, 32, 32, 0, 16, 35, 1190, 1024, 512, 1)
     SHAPE(32, 32, 16, 0, 16, 35, 1190, 512, 256, 2)
     SHAPE(16, 16, 16, 0, 16, 19, 342, 256, 64, 4)

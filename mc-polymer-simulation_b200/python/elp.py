@@ -34,7 +34,7 @@ class JobSpec(C.Structure):
 class Info(C.Structure):
     _fields_ = [("L", C.c_int32), ("N", C.c_int32), ("P", C.c_int32), ("periodic", C.c_int32),
                 ("tile", C.c_int32 * 3), ("ncol", C.c_int32), ("domains", C.c_int32), ("threads", C.c_int32),
-                ("smem_bytes", C.c_uint64), ("step", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("specialised", C.c_int32), ("smem_bytes", C.c_uint64), ("step", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
 EXPORTED = [
@@ -42,6 +42,9 @@ EXPORTED = [
     "elp_run_timed", "elp_sync", "elp_fetch_chains", "elp_write_tuv", "elp_check", "elp_get_info",
     "elp_get_state", "elp_set_state", "elp_accepted", "elp_destroy", "elp_transition_table",
     "elp_format_tuv", "elp_status_string", "elp_last_error",
+    "elp_batch_create", "elp_batch_size", "elp_batch_init_melts", "elp_batch_load_chains", "elp_batch_run",
+    "elp_batch_run_timed", "elp_batch_sync", "elp_batch_fetch_chains", "elp_batch_get_state", "elp_batch_check",
+    "elp_batch_accepted", "elp_batch_job_info", "elp_batch_destroy",
 ]
 
 _lib = None
@@ -76,6 +79,19 @@ def lib():
         "elp_format_tuv": (i32, [i32, i32, i32, vp, vp, vp, C.c_size_t, vp]),
         "elp_status_string": (C.c_char_p, [i32]),
         "elp_last_error": (C.c_char_p, []),
+        "elp_batch_create": (i32, [vp, i32, i32, vp]),
+        "elp_batch_size": (i32, [vp]),
+        "elp_batch_init_melts": (i32, [vp]),
+        "elp_batch_load_chains": (i32, [vp, i32, vp, vp, u64]),
+        "elp_batch_run": (i32, [vp, i64]),
+        "elp_batch_run_timed": (i32, [vp, i64, vp]),
+        "elp_batch_sync": (i32, [vp]),
+        "elp_batch_fetch_chains": (i32, [vp, i32, vp, vp]),
+        "elp_batch_get_state": (i32, [vp, i32, vp, vp]),
+        "elp_batch_check": (i32, [vp, i32, vp]),
+        "elp_batch_accepted": (i32, [vp, i32, vp]),
+        "elp_batch_job_info": (i32, [vp, i32, vp]),
+        "elp_batch_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -205,3 +221,75 @@ class Melt:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """Many melts advanced together on one GPU (an elp_batch)."""
+
+    def __init__(self, specs, device=0):
+        arr = (JobSpec * len(specs))()
+        for i, kw in enumerate(specs):
+            arr[i] = spec(**kw)
+        self.h = C.c_void_p()
+        check(lib().elp_batch_create(arr, len(specs), device, C.byref(self.h)))
+        self.n = lib().elp_batch_size(self.h)
+        self.infos = [self.info(j) for j in range(self.n)]
+
+    def info(self, j) -> Info:
+        i = Info()
+        check(lib().elp_batch_job_info(self.h, j, C.byref(i)))
+        return i
+
+    def init_melts(self):
+        check(lib().elp_batch_init_melts(self.h))
+
+    def load_chains(self, j, start, bonds, step=0):
+        start = np.ascontiguousarray(start, dtype=np.int32)
+        bonds = np.ascontiguousarray(bonds, dtype=np.uint8)
+        check(lib().elp_batch_load_chains(self.h, j, start.ctypes.data, bonds.ctypes.data, step))
+
+    def run(self, nsteps):
+        check(lib().elp_batch_run(self.h, nsteps))
+
+    def run_timed(self, nsteps) -> float:
+        ms = C.c_float()
+        check(lib().elp_batch_run_timed(self.h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        check(lib().elp_batch_sync(self.h))
+
+    def fetch(self, j):
+        i = self.infos[j]
+        start = np.zeros((i.P, 3), dtype=np.int32)
+        bonds = np.zeros((i.P, i.N), dtype=np.uint8)
+        check(lib().elp_batch_fetch_chains(self.h, j, start.ctypes.data, bonds.ctypes.data))
+        return start, bonds
+
+    def state(self, j):
+        i = self.infos[j]
+        w = np.zeros(i.L ** 3, dtype=np.uint32)
+        r = np.zeros((i.P, 4), dtype=np.uint32)
+        check(lib().elp_batch_get_state(self.h, j, w.ctypes.data, r.ctypes.data))
+        return w, r
+
+    def check(self, j) -> int:
+        code = C.c_int32()
+        check(lib().elp_batch_check(self.h, j, C.byref(code)))
+        return code.value
+
+    def accepted(self, j) -> int:
+        v = C.c_uint64()
+        check(lib().elp_batch_accepted(self.h, j, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().elp_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
