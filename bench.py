@@ -211,6 +211,10 @@ def run_elp(args, rank, world):
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps)
         if args.workload != "L256" and not args.no_l256:
             line["L256"] = l256_leg(elp, torch, dev, flush, args)
+        if not args.no_batched:
+            line["ensemble"] = batched_leg(elp, dev, args)
+        if not args.no_served:
+            line["served"] = served_leg(elp, dev, args)
     return line
 
 
@@ -269,6 +273,135 @@ def l256_leg(elp, torch, dev, flush, args):
                          "algorithmic_bytes_per_launch": algo_bytes(w), "traffic": profile_traffic("L256")}}
 
 
+# ---- batched ensemble (512 replicas) ------------------------------------------
+def _philox(ctr, key):
+    """Philox4x32-10 (Salmon et al., SC'11); used only to draw the synthetic mix."""
+    c0, c1, c2, c3 = ctr
+    k0, k1 = key
+    M = 0xFFFFFFFF
+    for _ in range(10):
+        p0 = 0xD2511F53 * c0
+        p1 = 0xCD9E8D57 * c2
+        c0, c1, c2, c3 = ((p1 >> 32) ^ c1 ^ k0) & M, p1 & M, ((p0 >> 32) ^ c3 ^ k1) & M, p0 & M
+        k0, k1 = (k0 + 0x9E3779B9) & M, (k1 + 0xBB67AE85) & M
+    return c0, c1, c2, c3
+
+
+def ensemble_mix(n=512, first_seed=1000, density=1.2):
+    """Replica i: seed 1000+i; L uniform on {16,24,32,48,64}; N log-uniform on
+    [50, 1000]; both drawn from Philox keyed by the replica's seed."""
+    import math
+    Ls = (16, 24, 32, 48, 64)
+    out = []
+    for i in range(n):
+        seed = first_seed + i
+        w = _philox((0, 0, 0, 0), (seed, 0xC0F4))
+        L = Ls[(w[0] * len(Ls)) >> 32]
+        u = w[1] / 2.0 ** 32
+        N = int(round(math.exp(math.log(50) + u * (math.log(1000) - math.log(50)))))
+        N = max(3, min(N, int(density * L ** 3 / 2)))
+        out.append(dict(L=L, N=N, seed=seed, density=density))
+    return out
+
+
+def batched_leg(elp, dev, args):
+    mix = ensemble_mix(args.replicas)
+    tuned = {}
+    for L in sorted({m["L"] for m in mix}):
+        ms = [m for m in mix if m["L"] == L]
+        sp, t = elp.autotune(copies=min(len(ms), 128), steps=10, device=dev, **dict(ms[0], steps_per_launch=100))
+        tuned[L] = sp
+    specs = []
+    for m in mix:
+        t = tuned[m["L"]]
+        specs.append(dict(m, periodic=t["periodic"], tile=t["tile"], ncol=t["ncol"],
+                          steps_per_launch=t["steps_per_launch"], device=dev))
+    moves = sum(sp["N"] * max(1, int(sp["density"] * sp["L"] ** 3 / sp["N"] + 0.5)) for sp in specs)
+    b = elp.Batch(specs, device=dev)
+    b.init_melts()
+    b.run(args.batch_warmup)
+    b.sync()
+    bms = b.run_timed(args.batch_steps)
+    batched = moves * args.batch_steps / (bms / 1e3)
+    # plain kernel, same mix, one replica at a time
+    pms, check_idx, same = 0.0, list(range(0, len(specs), max(1, len(specs) // 16))), True
+    for j, sp in enumerate(specs):
+        m = elp.Melt(**sp)
+        m.init_melt()
+        m.run(args.batch_warmup)
+        pms += m.run_timed(args.batch_steps)
+        if j in check_idx:
+            wa, ra = b.state(j)
+            wb, rb = m.state()
+            same = same and bool((wa == wb).all() and (ra == rb).all())
+        m.close()
+    plain = moves * args.batch_steps / (pms / 1e3)
+    b.close()
+    geoms = {str(L): {"periodic": t["periodic"], "tile": list(t["tile"]), "ncol": t["ncol"],
+                      "steps_per_launch": t["steps_per_launch"]} for L, t in tuned.items()}
+    return {"workload": f"{len(specs)} ring melts, L uniform on {{16,24,32,48,64}}, N log-uniform on [50,1000], "
+                        f"density 1.2, seeds 1000..{999 + len(specs)}",
+            "monomers": moves, "steps": args.batch_steps, "warmup": args.batch_warmup,
+            "batched": {"value": batched, "unit": UNIT, "ms": bms},
+            "plain": {"value": plain, "unit": UNIT, "ms": pms, "how": "each replica alone, same specs, sequential"},
+            "speedup": batched / plain, "batched_equals_plain_bits": same,
+            "replicas_compared": len(check_idx), "autotuned_geometry": geoms}
+
+
+# ---- served stream ------------------------------------------------------------
+def served_leg(elp, dev, args):
+    """Poisson arrivals into the continuous-batching server; job sizes drawn as
+    the ensemble mix plus 5 % L=128/N=1000 jobs; latency = done - submitted."""
+    import random
+    import threading
+    full = args.served_full
+    rate, dur = 200.0, (60.0 if full else args.served_seconds)
+    steps, dump = (10000, 1000) if full else (args.served_steps, args.served_dump)
+    rng = random.Random(20261203)
+    mix = ensemble_mix(4096, first_seed=50000)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.expovariate(rate)
+        if t >= dur:
+            break
+        arrivals.append(t)
+    jobs = []
+    for i, ta in enumerate(arrivals):
+        if rng.random() < 0.05:
+            jobs.append((ta, dict(L=128, N=1000, seed=90000 + i)))
+        else:
+            m = mix[i % len(mix)]
+            jobs.append((ta, dict(L=m["L"], N=m["N"], seed=m["seed"])))
+    srv = elp.Server(device=dev, hbm_budget=150 << 30, quantum=args.served_quantum)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for ta, kw in jobs:
+            d = ta - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            srv.submit(steps, dump_interval=dump, device=dev, **kw)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    srv.drain(3600)
+    wall = time.perf_counter() - t0
+    res = srv.poll(len(jobs) + 16)
+    srv.close()
+    lat = sorted(r["t_done"] - r["t_submit"] for r in res)
+    moves = sum(r["moves"] for r in res)
+    ok = all(r["status"] == 0 and r["integrity"] == 0 for r in res)
+    q = lambda f: lat[min(len(lat) - 1, int(f * len(lat)))]
+    makespan = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    return {"workload": f"Poisson arrivals {rate:.0f} jobs/s for {dur:.0f} s ({len(jobs)} jobs), sizes as the ensemble "
+                        f"mix plus 5% L=128/N=1000, {steps} steps each, dump every {dump} (rebuilt and copied to host, "
+                        f"no files), HBM budget 150 GB" + ("" if full else " [scaled-down stream]"),
+            "jobs": len(res), "all_ok": ok, "latency_s": {"p50": q(0.50), "p99": q(0.99), "max": lat[-1]},
+            "value": moves / makespan, "unit": UNIT, "makespan_s": makespan, "wall_s": wall,
+            "quantum": args.served_quantum}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -308,6 +441,16 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=5)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-l256", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--replicas", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--batch-warmup", type=int, default=20)
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-full", action="store_true")
+    ap.add_argument("--served-seconds", type=float, default=5.0)
+    ap.add_argument("--served-steps", type=int, default=1000)
+    ap.add_argument("--served-dump", type=int, default=250)
+    ap.add_argument("--served-quantum", type=int, default=50)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

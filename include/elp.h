@@ -165,6 +165,70 @@ elp_status elp_batch_accepted(elp_batch* b, int32_t job, uint64_t* accepted);
 elp_status elp_batch_job_info(const elp_batch* b, int32_t job, elp_info* info);
 void elp_batch_destroy(elp_batch* b);
 
+/* Autotuner: times the candidate domain geometries of `in` -- the whole box
+ * on chip (with 1, 10 or 100 steps per launch) and every tile shape that
+ * divides the box -- on `copies` copies of its initial melt run as one batch
+ * for `steps` steps, and returns the fastest as an explicit spec (periodic,
+ * tile, ncol, steps_per_launch filled in).  Whole-box domains have no tile
+ * walls, so a tiled shape is chosen only when it is over 1.5x faster.  The tile shape is part of a
+ * trajectory's definition: record the returned spec and reuse it; runs of the
+ * same spec give the same bits, alone or batched. */
+elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32_t steps, elp_job_spec* out,
+                        float* ms_per_step);
+
+/* ---- serving loop ------------------------------------------------------------
+ * Continuous batching of melt jobs on one GPU.  A scheduler thread runs ticks
+ * of `quantum` steps; between ticks it admits queued jobs whose device memory
+ * fits `hbm_budget`, so jobs that arrive while others run join the mix as
+ * memory frees up.  Lattices stay resident between dumps; a dump is copied on
+ * the device at the end of a tick and rebuilt + copied to pinned host memory
+ * on a side stream while the next tick computes; host threads write the TUV
+ * files `dump_dir/t=<step>_dev=0.res` (no files when dump_dir is NULL or "").
+ * A job's result depends only on its spec: alone or in any mix it gives the
+ * same bits (reported as a checksum of its final rings).  The reference has
+ * no serving mode (one job per process, gpupol2/gpupol2.c:14-70). */
+typedef struct elp_server elp_server;
+
+typedef struct elp_server_opts {
+    int32_t device;
+    uint64_t hbm_budget;      /* device bytes jobs may hold (state + one snapshot each) */
+    int32_t quantum;          /* steps per tick; job lengths and dump intervals are multiples */
+    int32_t io_threads;       /* host threads formatting and writing TUV files */
+    int32_t max_jobs;         /* resident job limit */
+} elp_server_opts;
+
+typedef struct elp_job_result {
+    uint64_t id;
+    int32_t status;           /* ELP_OK or the error that ended the job */
+    int32_t integrity;        /* CheckIntegrity code of the final state (0 ok) */
+    double t_submit, t_start, t_done;   /* seconds on the server clock */
+    uint64_t steps, moves;
+    uint32_t dumps;
+    uint64_t checksum;        /* FNV-1a of the final start[3P] and bonds[P*N] */
+    int32_t L, N, P;
+} elp_job_result;
+
+typedef struct elp_server_stats {
+    uint64_t submitted, completed, queued, resident, bytes_in_use;
+    double moves;             /* attempted monomer moves done so far */
+    double clock;             /* server clock (s) */
+    int32_t fatal;            /* non-zero: the scheduler stopped on this error */
+} elp_server_stats;
+
+void elp_server_default_opts(elp_server_opts* o);
+elp_status elp_server_create(const elp_server_opts* opts, elp_server** out);
+/* Queue a job: initial melt of `spec`, `nsteps` steps, a TUV dump every
+ * `dump_interval` steps (0: none) and at the end.  Thread-safe. */
+elp_status elp_server_submit(elp_server* s, const elp_job_spec* spec, int64_t nsteps, int64_t dump_interval,
+                             const char* dump_dir, uint64_t* id);
+/* Move up to `cap` finished jobs' results to `out`; *n receives the count. */
+elp_status elp_server_poll(elp_server* s, elp_job_result* out, int32_t cap, int32_t* n);
+elp_status elp_server_get_stats(elp_server* s, elp_server_stats* st);
+/* Wait until every submitted job has finished (or `timeout_s` passes). */
+elp_status elp_server_drain(elp_server* s, double timeout_s);
+/* Drop queued jobs, finish the ones on the GPU, stop. */
+void elp_server_destroy(elp_server* s);
+
 #ifdef __cplusplus
 }
 #endif

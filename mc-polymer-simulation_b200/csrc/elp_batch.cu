@@ -351,3 +351,78 @@ extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info
     info->device_bytes = b->device_bytes + b->wb.bytes;
     return ELP_OK;
 }
+
+// ---- autotuner ---------------------------------------------------------------
+// Candidate geometries for a melt: its whole box on chip (if that fits) with a
+// few steps-per-launch values, and every tile shape of the preference list
+// that divides the box.  Each is timed on `copies` copies of the initial melt
+// run as one batch (the best tile depends on how many melts share the GPU).
+extern "C" elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32_t steps, elp_job_spec* out,
+                                   float* ms_per_step)
+{
+    if (!in || !out || copies < 1 || steps < 1) return elp_fail(ELP_ERR_ARG, "bad argument");
+    std::vector<elp_job_spec> cand;
+    {
+        elp_job_spec s = *in;
+        s.periodic = 1;
+        s.tile[0] = s.tile[1] = s.tile[2] = 0;
+        s.ncol = 0;
+        int P;
+        elp_geometry g;
+        if (elp_resolve_spec(&s, &P, &g) == ELP_OK) {
+            const int spls[] = {1, 10, 100};
+            for (int spl : spls) {
+                if (spl > steps) continue;
+                s.steps_per_launch = spl;
+                cand.push_back(s);
+            }
+        }
+    }
+    static const int tiles[][3] = {{32, 32, 32}, {48, 24, 24}, {32, 32, 16}, {24, 24, 24}, {32, 16, 16},
+                                   {16, 16, 16}, {40, 20, 20}, {20, 20, 20}, {16, 16, 8}};
+    for (const auto& t : tiles) {
+        elp_job_spec s = *in;
+        s.periodic = 0;
+        s.tile[0] = t[0]; s.tile[1] = t[1]; s.tile[2] = t[2];
+        s.ncol = 0;
+        s.steps_per_launch = 1;
+        int P;
+        elp_geometry g;
+        if (in->L % t[0] || in->L % t[1] || in->L % t[2]) continue;
+        if (elp_resolve_spec(&s, &P, &g) != ELP_OK) continue;
+        cand.push_back(s);
+    }
+    if (cand.empty()) return elp_fail(ELP_ERR_ARG, "no candidate geometry for L=%d", in->L);
+    float best = -1.f, best_score = 0.f;
+    for (const elp_job_spec& c : cand) {
+        std::vector<elp_job_spec> specs((size_t)copies, c);
+        for (int k = 0; k < copies; k++) specs[(size_t)k].seed = c.seed + (uint32_t)k;
+        elp_batch* b = nullptr;
+        if (elp_batch_create(specs.data(), copies, in->device, &b) != ELP_OK) continue;
+        float ms = 0.f;
+        elp_status st = elp_batch_init_melts(b);
+        if (st == ELP_OK) st = elp_batch_run(b, steps);  // warm-up (and graph capture)
+        if (st == ELP_OK) st = elp_batch_run_timed(b, steps, &ms);
+        elp_batch_destroy(b);
+        if (st != ELP_OK) continue;
+        // Whole-box domains have no tile walls (no rejected boundary moves), so
+        // a tiled shape must be clearly faster to be preferred.
+        const float per = ms / (float)steps;
+        const float score = c.periodic == 1 ? per / 1.5f : per;
+        if (best < 0.f || score < best_score) {
+            best = per;
+            best_score = score;
+            *out = c;
+        }
+    }
+    if (best < 0.f) return elp_fail(ELP_ERR_CUDA, "no candidate geometry could be run");
+    // make the choice explicit
+    int P;
+    elp_geometry g;
+    elp_resolve_spec(out, &P, &g);
+    out->periodic = g.periodic;
+    out->tile[0] = g.tx; out->tile[1] = g.ty; out->tile[2] = g.tz;
+    out->ncol = g.ncol;
+    if (ms_per_step) *ms_per_step = best;
+    return ELP_OK;
+}

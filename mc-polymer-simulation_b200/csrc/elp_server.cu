@@ -1,0 +1,618 @@
+// elp_server.cu -- the serving loop: continuous batching of melt jobs.
+//
+// Jobs (a melt spec, a step count, a dump interval) arrive at any time.  A
+// scheduler thread runs ticks of `quantum` steps.  Between ticks it admits
+// queued jobs whose device memory fits the HBM budget, places them in the
+// group of their domain geometry (elp_group.h) and retires finished ones, so
+// requests that arrive while others are on the GPU join the running mix as
+// memory frees up.  Lattices stay resident between dumps.  At a dump the
+// job's state is copied device-to-device at the end of the tick; rebuilding
+// the rings and the device-to-host copy into pinned memory then run on a side
+// stream while the next tick computes, and host I/O threads format the TUV
+// text.  A job follows the same trajectory alone, in any mix, or through the
+// single-melt API: its kernel, counters and geometry depend only on its spec.
+//
+// The reference runs one fixed job per process (gpupol2/gpupol2.c:14-70 with
+// a synchronous dump per interval, gpupol2/gpupol_cuda.cu:52-76); it has no
+// serving mode.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <sys/stat.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "elp_common.h"
+#include "elp_group.h"
+#include "elp_kernels.h"
+
+namespace {
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n)
+{
+    const uint8_t* b = (const uint8_t*)p;
+    for (size_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 0x100000001b3ULL;
+    }
+    return h;
+}
+
+struct SJob {
+    uint64_t id = 0;
+    elp_job_spec spec;
+    elp_geometry g;
+    int P = 0;
+    int64_t nsteps = 0, dump_interval = 0, done_steps = 0;
+    std::string dir;
+    double t_submit = 0, t_start = 0, t_done = 0;
+    uint32_t dumps = 0;
+    size_t bytes = 0;
+    uint32_t* lat = nullptr;
+    uint32_t* rec = nullptr;
+    int group = -1, index = -1;
+    elp_status status = ELP_OK;
+    int integrity = -1;
+    uint64_t checksum = 0;
+    std::string error;
+};
+
+// A snapshot on its way to the host.
+struct Snap {
+    SJob* job = nullptr;
+    int64_t step = 0;
+    bool final = false;
+    uint32_t* d_lat = nullptr;
+    uint32_t* d_rec = nullptr;
+};
+
+struct IOWork {
+    SJob* job;
+    int64_t step;
+    bool final;
+    std::vector<int32_t> start;
+    std::vector<uint8_t> bonds;
+};
+
+struct SGroup {
+    std::tuple<int, int, int, int, int, int> key;
+    elp_group G;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    std::vector<SJob*> members;
+    bool dirty = false;
+};
+
+}  // namespace
+
+struct elp_server {
+    elp_server_opts o;
+    int nsm = 148;
+    std::chrono::steady_clock::time_point t0;
+    uint32_t* d_table = nullptr;
+    uint32_t* d_err = nullptr;            // 64 groups x 4 words
+    unsigned long long* d_acc = nullptr;  // accepted moves (all jobs together)
+    cudaStream_t side = nullptr;
+    elp_walk_bufs wb;
+
+    std::mutex mu;
+    std::condition_variable cv, cv_done;
+    std::deque<SJob*> queue;
+    std::vector<SJob*> finished;          // results not yet polled
+    uint64_t next_id = 1;
+    std::atomic<bool> stop{false};
+    std::atomic<bool> io_stop{false};     // set after the scheduler has finished
+    uint64_t submitted = 0, completed = 0;
+    size_t bytes_in_use = 0;
+    double moves_done = 0;
+    elp_status fatal = ELP_OK;
+    std::string fatal_msg;
+
+    std::vector<std::unique_ptr<SGroup>> groups;
+    std::vector<SJob*> resident;
+    std::vector<Snap> pending;            // snapshots taken at the end of the last tick
+
+    std::mutex io_mu;
+    std::condition_variable io_cv;
+    std::deque<IOWork*> io_q;
+    std::vector<std::thread> io_threads;
+    std::atomic<int> io_busy{0};
+    std::thread sched;
+
+    double now() const
+    {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+static void io_worker(elp_server* s)
+{
+    for (;;) {
+        IOWork* w = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->io_mu);
+            s->io_cv.wait(lk, [&] { return s->io_stop.load() || !s->io_q.empty(); });
+            if (s->io_q.empty()) return;
+            w = s->io_q.front();
+            s->io_q.pop_front();
+        }
+        SJob* j = w->job;
+        const int L = j->g.L, N = j->spec.N, P = j->P;
+        if (!j->dir.empty()) {
+            size_t len = 0;
+            elp_format_tuv(L, N, P, w->start.data(), w->bonds.data(), nullptr, 0, &len);
+            std::string text(len + 1, '\0');
+            elp_format_tuv(L, N, P, w->start.data(), w->bonds.data(), &text[0], len + 1, &len);
+            char path[4096];
+            snprintf(path, sizeof(path), "%s/t=%lld_dev=0.res", j->dir.c_str(), (long long)w->step);
+            FILE* f = fopen(path, "wb");
+            if (f) {
+                fwrite(text.data(), 1, len, f);
+                fclose(f);
+            }
+        }
+        if (w->final) {
+            uint64_t h = 0xcbf29ce484222325ULL;
+            h = fnv1a(h, w->start.data(), w->start.size() * sizeof(int32_t));
+            h = fnv1a(h, w->bonds.data(), w->bonds.size());
+            j->checksum = h;
+            std::lock_guard<std::mutex> lk(s->mu);
+            j->t_done = s->now();
+            s->finished.push_back(j);
+            s->completed++;
+            s->cv_done.notify_all();
+        }
+        delete w;
+        s->io_busy--;
+    }
+}
+
+static SGroup* group_for(elp_server* s, SJob* j)
+{
+    auto key = std::make_tuple(j->g.periodic, j->g.L, j->g.tx, j->g.ty, j->g.tz, j->g.ncol);
+    for (auto& gp : s->groups)
+        if (gp->key == key) return gp.get();
+    if (s->groups.size() >= 64) return nullptr;
+    std::unique_ptr<SGroup> gp(new SGroup());
+    gp->key = key;
+    if (cudaStreamCreateWithFlags(&gp->s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    if (cudaEventCreateWithFlags(&gp->ev, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    if (elp_group_init(&gp->G, j->g, s->nsm, 0, s->o.quantum, s->d_table, s->d_err + 4 * s->groups.size(), gp->s) !=
+        cudaSuccess)
+        return nullptr;
+    gp->G.graph_steps = s->o.quantum;
+    s->groups.push_back(std::move(gp));
+    return s->groups.back().get();
+}
+
+static void fail_job(elp_server* s, SJob* j, elp_status st, const char* msg)
+{
+    j->status = st;
+    j->error = msg;
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->t_done = s->now();
+    s->finished.push_back(j);
+    s->completed++;
+    s->cv_done.notify_all();
+}
+
+// Admit queued jobs that fit the budget; returns false on a fatal CUDA error.
+static bool admit(elp_server* s)
+{
+    for (;;) {
+        SJob* j = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->queue.empty()) return true;
+            SJob* c = s->queue.front();
+            if (s->resident.size() >= (size_t)s->o.max_jobs) return true;
+            if (s->bytes_in_use + c->bytes > s->o.hbm_budget && !s->resident.empty()) return true;
+            s->queue.pop_front();
+            j = c;
+        }
+        if (j->bytes > s->o.hbm_budget) {
+            fail_job(s, j, ELP_ERR_BUSY, "job needs more device memory than the server budget");
+            continue;
+        }
+        SGroup* gp = group_for(s, j);
+        if (!gp) {
+            fail_job(s, j, ELP_ERR_CUDA, "cannot create a group for the job");
+            continue;
+        }
+        const size_t S = (size_t)j->g.L * j->g.L * j->g.L;
+        if (cudaMallocAsync((void**)&j->lat, S * 4, gp->s) != cudaSuccess ||
+            cudaMallocAsync((void**)&j->rec, (size_t)j->P * ELP_REC_WORDS * 4, gp->s) != cudaSuccess) {
+            fail_job(s, j, ELP_ERR_NOMEM, "device allocation failed");
+            continue;
+        }
+        std::vector<int32_t> start((size_t)j->P * 3);
+        std::vector<uint8_t> bonds((size_t)j->P * j->spec.N);
+        std::vector<uint32_t> lat(S), rec((size_t)j->P * ELP_REC_WORDS);
+        if (elp_initial_chains(j->g.L, j->spec.N, j->P, start.data(), bonds.data()) ||
+            elp_chains_to_sites(j->g.L, j->spec.N, j->P, start.data(), bonds.data(), lat.data(), rec.data())) {
+            cudaFreeAsync(j->lat, gp->s);
+            cudaFreeAsync(j->rec, gp->s);
+            fail_job(s, j, ELP_ERR_ARG, "initial melt does not fit the box");
+            continue;
+        }
+        cudaMemcpyAsync(j->lat, lat.data(), S * 4, cudaMemcpyHostToDevice, gp->s);
+        cudaMemcpyAsync(j->rec, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice, gp->s);
+        if (cudaStreamSynchronize(gp->s) != cudaSuccess) return false;
+        for (size_t g = 0; g < s->groups.size(); g++)
+            if (s->groups[g].get() == gp) j->group = (int)g;
+        gp->members.push_back(j);
+        gp->dirty = true;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->bytes_in_use += j->bytes;
+        }
+        j->t_start = s->now();
+        s->resident.push_back(j);
+    }
+}
+
+static bool rebuild(elp_server* s, SGroup* gp)
+{
+    elp_group& G = gp->G;
+    // absolute steps of the members are kept in the jobs; rebuild the table
+    G.jobs.clear();
+    G.N.clear();
+    for (size_t i = 0; i < gp->members.size(); i++) {
+        SJob* j = gp->members[i];
+        j->index = (int)i;
+        elp_group_add(&G, j->lat, j->rec, s->d_acc, j->spec.N, j->P, j->spec.seed, j->spec.salt,
+                      (uint64_t)j->done_steps);
+    }
+    gp->dirty = false;
+    if (gp->members.empty()) return true;
+    return elp_group_commit(&G) == cudaSuccess;
+}
+
+// Rebuild rings of a snapshot on the side stream and hand them to I/O.
+static bool drain_snap(elp_server* s, Snap& sn)
+{
+    SJob* j = sn.job;
+    IOWork* w = new IOWork();
+    w->job = j;
+    w->step = sn.step;
+    w->final = sn.final;
+    w->start.resize((size_t)j->P * 3);
+    w->bonds.resize((size_t)j->P * j->spec.N);
+    elp_status st = elp_fetch_rings(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, &s->wb, w->start.data(),
+                                    w->bonds.data(), s->side);
+    if (sn.final && st == ELP_OK) {
+        int32_t code = -1;
+        if (elp_check_melt(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, &s->wb, &code, s->side) == ELP_OK)
+            j->integrity = code;
+    }
+    cudaFreeAsync(sn.d_lat, s->side);
+    cudaFreeAsync(sn.d_rec, s->side);
+    if (st != ELP_OK) {
+        delete w;
+        if (sn.final) fail_job(s, j, st, elp_last_error());
+        return cudaStreamSynchronize(s->side) == cudaSuccess;
+    }
+    s->io_busy++;
+    {
+        std::lock_guard<std::mutex> lk(s->io_mu);
+        s->io_q.push_back(w);
+    }
+    s->io_cv.notify_one();
+    return true;
+}
+
+static void scheduler(elp_server* s)
+{
+    cudaSetDevice(s->o.device);
+    const int64_t Q = s->o.quantum;
+    for (;;) {
+        if (!admit(s)) break;
+        for (auto& gp : s->groups)
+            if (gp->dirty && !rebuild(s, gp.get())) {
+                s->fatal = ELP_ERR_CUDA;
+                s->fatal_msg = "group rebuild failed";
+            }
+        if (s->fatal) break;
+        // one tick on every group with members
+        bool any = false;
+        for (auto& gp : s->groups) {
+            if (gp->members.empty()) continue;
+            any = true;
+            if (elp_group_run(&gp->G, Q) != cudaSuccess || cudaEventRecord(gp->ev, gp->s) != cudaSuccess) {
+                s->fatal = ELP_ERR_CUDA;
+                s->fatal_msg = "launch failed";
+            }
+        }
+        // while the tick computes: finish the snapshots of the previous tick
+        for (Snap& sn : s->pending)
+            if (!drain_snap(s, sn)) {
+                s->fatal = ELP_ERR_CUDA;
+                s->fatal_msg = "snapshot failed";
+            }
+        s->pending.clear();
+        if (s->fatal) break;
+        if (!any) {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (s->stop.load() && s->queue.empty()) break;
+            s->cv.wait_for(lk, std::chrono::milliseconds(2));
+            continue;
+        }
+        // tick done: bookkeeping, snapshots, retirements
+        std::vector<SJob*> keep;
+        for (auto& gp : s->groups) {
+            if (gp->members.empty()) continue;
+            if (cudaEventSynchronize(gp->ev) != cudaSuccess) {
+                s->fatal = ELP_ERR_CUDA;
+                s->fatal_msg = "tick failed";
+                break;
+            }
+            std::vector<SJob*> stay;
+            for (SJob* j : gp->members) {
+                j->done_steps += Q;
+                const bool fin = j->done_steps >= j->nsteps;
+                const bool dump = j->dump_interval > 0 && j->done_steps % j->dump_interval == 0;
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    s->moves_done += (double)Q * j->spec.N * j->P;
+                }
+                if (dump || fin) {
+                    Snap sn;
+                    sn.job = j;
+                    sn.step = j->done_steps;
+                    sn.final = fin;
+                    const size_t S = (size_t)j->g.L * j->g.L * j->g.L;
+                    if (cudaMallocAsync((void**)&sn.d_lat, S * 4, gp->s) != cudaSuccess ||
+                        cudaMallocAsync((void**)&sn.d_rec, (size_t)j->P * ELP_REC_WORDS * 4, gp->s) != cudaSuccess) {
+                        s->fatal = ELP_ERR_NOMEM;
+                        s->fatal_msg = "snapshot allocation failed";
+                        break;
+                    }
+                    cudaMemcpyAsync(sn.d_lat, j->lat, S * 4, cudaMemcpyDeviceToDevice, gp->s);
+                    cudaMemcpyAsync(sn.d_rec, j->rec, (size_t)j->P * ELP_REC_WORDS * 4, cudaMemcpyDeviceToDevice, gp->s);
+                    if (dump) j->dumps++;
+                    s->pending.push_back(sn);
+                }
+                if (fin) {
+                    cudaFreeAsync(j->lat, gp->s);
+                    cudaFreeAsync(j->rec, gp->s);
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    s->bytes_in_use -= j->bytes;
+                    gp->dirty = true;
+                } else {
+                    stay.push_back(j);
+                }
+            }
+            gp->members.swap(stay);
+            // snapshot copies must land before the side stream reads them
+            cudaEventRecord(gp->ev, gp->s);
+            cudaStreamWaitEvent(s->side, gp->ev, 0);
+        }
+        s->resident.clear();
+        for (auto& gp : s->groups)
+            for (SJob* j : gp->members) s->resident.push_back(j);
+        uint32_t flags[64 * 4];
+        if (cudaMemcpy(flags, s->d_err, sizeof(flags), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            s->fatal = ELP_ERR_CUDA;
+            s->fatal_msg = "cannot read device error flags";
+        }
+        for (size_t g = 0; g < s->groups.size() && !s->fatal; g++)
+            if (flags[4 * g]) {
+                s->fatal = ELP_ERR_STATE;
+                s->fatal_msg = "a domain held more monomer-0 runs than its label table";
+            }
+        if (s->fatal) break;
+    }
+    for (Snap& sn : s->pending) drain_snap(s, sn);
+    s->pending.clear();
+    cudaStreamSynchronize(s->side);
+    if (s->fatal) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (SJob* j : s->resident) {
+            j->status = s->fatal;
+            j->error = s->fatal_msg;
+            j->t_done = s->now();
+            s->finished.push_back(j);
+            s->completed++;
+        }
+        s->resident.clear();
+        for (SJob* j : s->queue) {
+            j->status = s->fatal;
+            j->error = s->fatal_msg;
+            s->finished.push_back(j);
+            s->completed++;
+        }
+        s->queue.clear();
+        s->cv_done.notify_all();
+    }
+}
+
+extern "C" void elp_server_default_opts(elp_server_opts* o)
+{
+    memset(o, 0, sizeof(*o));
+    o->device = 0;
+    o->hbm_budget = 150ull << 30;
+    o->quantum = 100;
+    o->io_threads = 4;
+    o->max_jobs = 4096;
+}
+
+extern "C" elp_status elp_server_create(const elp_server_opts* opts, elp_server** out)
+{
+    if (!opts || !out) return elp_fail(ELP_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (opts->quantum < 1 || opts->io_threads < 1 || opts->max_jobs < 1)
+        return elp_fail(ELP_ERR_ARG, "quantum, io_threads and max_jobs must be positive");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return elp_fail(ELP_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (opts->device < 0 || opts->device >= ndev) return elp_fail(ELP_ERR_ARG, "device %d not present", opts->device);
+    ELP_CUDA_TRY(cudaSetDevice(opts->device));
+    elp_server* s = new (std::nothrow) elp_server();
+    if (!s) return elp_fail(ELP_ERR_NOMEM, "host allocation failed");
+    s->o = *opts;
+    s->t0 = std::chrono::steady_clock::now();
+    if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, opts->device) != cudaSuccess) s->nsm = 148;
+    uint8_t tab[4096];
+    elp_build_table(tab);
+    if (cudaMalloc((void**)&s->d_table, 4096) != cudaSuccess || cudaMalloc((void**)&s->d_err, 64 * 16) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_acc, 8) != cudaSuccess ||
+        cudaMemcpy(s->d_table, tab, 4096, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(s->d_err, 0, 64 * 16) != cudaSuccess || cudaMemset(s->d_acc, 0, 8) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc);
+        delete s;
+        return elp_fail(ELP_ERR_CUDA, "server set-up failed");
+    }
+    for (int i = 0; i < opts->io_threads; i++) s->io_threads.emplace_back(io_worker, s);
+    s->sched = std::thread(scheduler, s);
+    *out = s;
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_server_submit(elp_server* s, const elp_job_spec* spec, int64_t nsteps, int64_t dump_interval,
+                                        const char* dump_dir, uint64_t* id)
+{
+    if (!s || !spec) return elp_fail(ELP_ERR_ARG, "null argument");
+    if (nsteps < 1) return elp_fail(ELP_ERR_ARG, "a job needs at least one step");
+    const int64_t Q = s->o.quantum;
+    if (nsteps % Q) return elp_fail(ELP_ERR_ARG, "steps must be a multiple of the quantum (%lld)", (long long)Q);
+    if (dump_interval < 0 || (dump_interval && dump_interval % Q))
+        return elp_fail(ELP_ERR_ARG, "dump interval must be a multiple of the quantum (%lld)", (long long)Q);
+    SJob* j = new (std::nothrow) SJob();
+    if (!j) return elp_fail(ELP_ERR_NOMEM, "host allocation failed");
+    j->spec = *spec;
+    j->spec.steps_per_launch = (int32_t)Q;
+    elp_status st = elp_resolve_spec(&j->spec, &j->P, &j->g);
+    if (st) {
+        delete j;
+        return st;
+    }
+    j->nsteps = nsteps;
+    j->dump_interval = dump_interval;
+    if (dump_dir && dump_dir[0]) {
+        j->dir = dump_dir;
+        mkdir(dump_dir, 0755);
+    }
+    const size_t S = (size_t)j->g.L * j->g.L * j->g.L;
+    j->bytes = 2 * (S * 4 + (size_t)j->P * ELP_REC_WORDS * 4);  // resident state + one snapshot
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop.load()) {
+        delete j;
+        return elp_fail(ELP_ERR_STATE, "server is shutting down");
+    }
+    j->id = s->next_id++;
+    j->t_submit = s->now();
+    s->queue.push_back(j);
+    s->submitted++;
+    s->cv.notify_all();
+    if (id) *id = j->id;
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_server_poll(elp_server* s, elp_job_result* out, int32_t cap, int32_t* n)
+{
+    if (!s || !n || (cap > 0 && !out)) return elp_fail(ELP_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    int k = 0;
+    while (k < cap && !s->finished.empty()) {
+        SJob* j = s->finished.front();
+        s->finished.erase(s->finished.begin());
+        elp_job_result& r = out[k++];
+        memset(&r, 0, sizeof(r));
+        r.id = j->id;
+        r.status = j->status;
+        r.integrity = j->integrity;
+        r.t_submit = j->t_submit;
+        r.t_start = j->t_start;
+        r.t_done = j->t_done;
+        r.steps = (uint64_t)j->done_steps;
+        r.moves = (uint64_t)j->done_steps * (uint64_t)j->spec.N * (uint64_t)j->P;
+        r.dumps = j->dumps;
+        r.checksum = j->checksum;
+        r.L = j->g.L;
+        r.N = j->spec.N;
+        r.P = j->P;
+        delete j;
+    }
+    *n = k;
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_server_get_stats(elp_server* s, elp_server_stats* st)
+{
+    if (!s || !st) return elp_fail(ELP_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    memset(st, 0, sizeof(*st));
+    st->submitted = s->submitted;
+    st->completed = s->completed;
+    st->queued = s->queue.size();
+    st->resident = s->resident.size();
+    st->bytes_in_use = s->bytes_in_use;
+    st->moves = s->moves_done;
+    st->clock = s->now();
+    st->fatal = s->fatal;
+    return ELP_OK;
+}
+
+extern "C" elp_status elp_server_drain(elp_server* s, double timeout_s)
+{
+    if (!s) return elp_fail(ELP_ERR_ARG, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                  [&] { return s->completed == s->submitted || s->fatal; });
+    if (s->fatal) return elp_fail(s->fatal, "server stopped: %s", s->fatal_msg.c_str());
+    if (!ok) return elp_fail(ELP_ERR_BUSY, "jobs still running after %.1f s", timeout_s);
+    return ELP_OK;
+}
+
+extern "C" void elp_server_destroy(elp_server* s)
+{
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        for (SJob* j : s->queue) delete j;
+        s->queue.clear();
+        s->cv.notify_all();
+    }
+    // finish the jobs already on the GPU, then stop
+    while (true) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->resident.empty() || s->fatal) break;
+        }
+        std::this_thread::sleep_for(std::chrono::milliseconds(5));
+    }
+    if (s->sched.joinable()) s->sched.join();
+    while (s->io_busy.load() > 0) std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    {
+        std::lock_guard<std::mutex> lk(s->io_mu);
+        s->io_stop = true;
+    }
+    s->io_cv.notify_all();
+    for (auto& t : s->io_threads) t.join();
+    cudaSetDevice(s->o.device);
+    for (auto& gp : s->groups) {
+        cudaStreamSynchronize(gp->s);
+        elp_group_free(&gp->G);
+        cudaStreamDestroy(gp->s);
+        cudaEventDestroy(gp->ev);
+    }
+    elp_walk_bufs_free(&s->wb);
+    cudaStreamDestroy(s->side);
+    cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc);
+    for (SJob* j : s->finished) delete j;
+    delete s;
+}

@@ -363,10 +363,10 @@ extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
     if (g.tx == X_ && g.ty == Y_ && g.tz == Z_ && g.periodic == PER_ && g.ncol == NC_ && l->sx == SX_ &&       \
         l->sxy == SXY_)                                                                                        \
         return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_>(l, s);
-    SHAPE(32, 32, 32, 0, 16, 35, 1190, 1024, 512, 1)
-    SHAPE(32, 32, 16, 0, 16, 35, 1190, 512, 256, 2)
-    SHAPE(16, 16, 16, 0, 16, 19, 342, 256, 64, 4)
-    SHAPE(48, 24, 24, 0, 16, 51, 1326, 1024, 448, 1)
+    SHAPE(32, 32, 32, 0, 16, 35, 1190, 2048, 512, 1)
+    SHAPE(32, 32, 16, 0, 16, 35, 1190, 1024, 256, 2)
+    SHAPE(16, 16, 16, 0, 16, 19, 342, 512, 64, 4)
+    SHAPE(48, 24, 24, 0, 16, 51, 1326, 2048, 448, 1)
     SHAPE(16, 16, 16, 1, 16, 16, 256, 2048, 64, 1)
     SHAPE(32, 32, 32, 1, 16, 33, 1056, 2048, 512, 1)
     SHAPE(24, 24, 24, 1, 24, 24, 576, 2048, 160, 1)

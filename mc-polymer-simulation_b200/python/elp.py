@@ -44,7 +44,9 @@ EXPORTED = [
     "elp_format_tuv", "elp_status_string", "elp_last_error",
     "elp_batch_create", "elp_batch_size", "elp_batch_init_melts", "elp_batch_load_chains", "elp_batch_run",
     "elp_batch_run_timed", "elp_batch_sync", "elp_batch_fetch_chains", "elp_batch_get_state", "elp_batch_check",
-    "elp_batch_accepted", "elp_batch_job_info", "elp_batch_destroy",
+    "elp_batch_accepted", "elp_batch_job_info", "elp_batch_destroy", "elp_autotune",
+    "elp_server_default_opts", "elp_server_create", "elp_server_submit", "elp_server_poll", "elp_server_get_stats",
+    "elp_server_drain", "elp_server_destroy",
 ]
 
 _lib = None
@@ -92,6 +94,14 @@ def lib():
         "elp_batch_accepted": (i32, [vp, i32, vp]),
         "elp_batch_job_info": (i32, [vp, i32, vp]),
         "elp_batch_destroy": (None, [vp]),
+        "elp_autotune": (i32, [vp, i32, i32, vp, vp]),
+        "elp_server_default_opts": (None, [vp]),
+        "elp_server_create": (i32, [vp, vp]),
+        "elp_server_submit": (i32, [vp, vp, i64, i64, C.c_char_p, vp]),
+        "elp_server_poll": (i32, [vp, vp, i32, vp]),
+        "elp_server_get_stats": (i32, [vp, vp]),
+        "elp_server_drain": (i32, [vp, C.c_double]),
+        "elp_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -132,6 +142,18 @@ def spec(L=32, N=100, P=0, density=1.2, seed=1, salt=0, periodic=-1, tile=(0, 0,
     s.tile[0], s.tile[1], s.tile[2] = tile
     s.ncol, s.device, s.steps_per_launch, s.kernel = ncol, device, steps_per_launch, kernel
     return s
+
+
+def autotune(copies=1, steps=20, **kw):
+    """Fastest domain geometry for a melt (see elp_autotune).  Returns
+    (spec dict, ms per step)."""
+    src = spec(**kw)
+    out = JobSpec()
+    ms = C.c_float()
+    check(lib().elp_autotune(C.byref(src), copies, steps, C.byref(out), C.byref(ms)))
+    d = dict(kw)
+    d.update(periodic=out.periodic, tile=tuple(out.tile), ncol=out.ncol, steps_per_launch=out.steps_per_launch)
+    return d, ms.value
 
 
 class Melt:
@@ -286,6 +308,74 @@ class Batch:
     def close(self):
         if getattr(self, "h", None) and self.h.value:
             lib().elp_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget", C.c_uint64), ("quantum", C.c_int32),
+                ("io_threads", C.c_int32), ("max_jobs", C.c_int32)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int32), ("integrity", C.c_int32), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_done", C.c_double), ("steps", C.c_uint64), ("moves", C.c_uint64),
+                ("dumps", C.c_uint32), ("checksum", C.c_uint64), ("L", C.c_int32), ("N", C.c_int32),
+                ("P", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("queued", C.c_uint64),
+                ("resident", C.c_uint64), ("bytes_in_use", C.c_uint64), ("moves", C.c_double),
+                ("clock", C.c_double), ("fatal", C.c_int32)]
+
+
+def ring_checksum(start, bonds) -> int:
+    """FNV-1a of start[3P] (int32) then bonds[P*N], as the server reports."""
+    h = 0xCBF29CE484222325
+    for b in np.ascontiguousarray(start, dtype=np.int32).tobytes() + np.ascontiguousarray(bonds, np.uint8).tobytes():
+        h = ((h ^ b) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+class Server:
+    """Continuous-batching job server on one GPU (an elp_server)."""
+
+    def __init__(self, device=0, hbm_budget=150 << 30, quantum=100, io_threads=4, max_jobs=4096):
+        o = ServerOpts()
+        lib().elp_server_default_opts(C.byref(o))
+        o.device, o.hbm_budget, o.quantum, o.io_threads, o.max_jobs = device, hbm_budget, quantum, io_threads, max_jobs
+        self.h = C.c_void_p()
+        check(lib().elp_server_create(C.byref(o), C.byref(self.h)))
+
+    def submit(self, nsteps, dump_interval=0, dump_dir=None, **kw) -> int:
+        jid = C.c_uint64()
+        d = dump_dir.encode() if dump_dir else None
+        check(lib().elp_server_submit(self.h, C.byref(spec(**kw)), nsteps, dump_interval, d, C.byref(jid)))
+        return jid.value
+
+    def poll(self, cap=1024):
+        out = (JobResult * cap)()
+        n = C.c_int32()
+        check(lib().elp_server_poll(self.h, out, cap, C.byref(n)))
+        return [{f: getattr(out[i], f) for f, _ in JobResult._fields_} for i in range(n.value)]
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().elp_server_get_stats(self.h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def drain(self, timeout=600.0):
+        check(lib().elp_server_drain(self.h, timeout))
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().elp_server_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
