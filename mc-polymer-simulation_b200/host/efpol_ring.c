@@ -1,0 +1,166 @@
+/*
+ * efpol_ring -- drop-in replacement of the reference's CPU program efpol_ring
+ * (cpupol/efpol.c:4-114) running the ELP sweep on the GPU.
+ *
+ *   efpol_ring SEED DIR DENSITY TIME INTERVAL NMONO DBLSTEP L MODEL
+ *
+ * Same arguments (do_run.sh:343), same output tree and file names:
+ * DIR/N_<N>/t=<t>_dev=0.res every INTERVAL steps from t=0, a last file at
+ * ceil(TIME/INTERVAL)*INTERVAL, and DIR/N_<N>/simulation_settings.txt with
+ * the keys of cpupol/efpol_io.c:111-140.  Like efpol, L is rounded up to a
+ * power of two (efpol.c:53-58) and the ring count is GetNPol.  Exit codes as
+ * efpol: 0 ok, 192 integrity failure, 193 unknown/unsupported model.
+ * Supported: MODEL sl_equal and DBLSTEP 0 (hierarchical doubling is not
+ * provided).  "Executable = efpol" is written because the dynamics are
+ * efpol's single-monomer dynamics (same move table and attempt rate).
+ */
+#include <errno.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <time.h>
+
+#include "elp.h"
+
+static int mkdir_p(const char* path)
+{
+    char buf[4096];
+    size_t n = strlen(path);
+    if (n == 0 || n >= sizeof(buf)) return -1;
+    memcpy(buf, path, n + 1);
+    for (size_t i = 1; i <= n; i++) {
+        if (buf[i] == '/' || buf[i] == '\0') {
+            char c = buf[i];
+            buf[i] = '\0';
+            if (mkdir(buf, 0755) && errno != EEXIST) return -1;
+            buf[i] = c;
+        }
+    }
+    return 0;
+}
+
+static double now_s(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+static int die(elp_status st, int code)
+{
+    fprintf(stderr, "efpol_ring: %s: %s\n", elp_status_string(st), elp_last_error());
+    return code;
+}
+
+int main(int argc, char** argv)
+{
+    unsigned seed = 37249131u;
+    const char* dir = "./data/test";
+    double density = 1.0;
+    long tmax = 1000, interval = 100;
+    int nmono = 4, dbl = 0, lstart = 16;
+    const char* model = "sl_quad";
+    if (argc <= 8) {
+        printf("In testing mode, using defaults\n");
+    } else {
+        seed = (unsigned)strtoul(argv[1], 0, 10);
+        dir = argv[2];
+        density = atof(argv[3]);
+        tmax = (long)atof(argv[4]);
+        interval = (long)atof(argv[5]);
+        nmono = atoi(argv[6]);
+        dbl = atoi(argv[7]);
+        lstart = atoi(argv[8]);
+        model = argc > 9 ? argv[9] : "";
+    }
+    if (strcmp(model, "sl_equal") != 0) {
+        if (strcmp(model, "sl_double") && strcmp(model, "sl_quad")) {
+            printf("Unknown polymer model, aborting!\n");
+            return 193;
+        }
+        fprintf(stderr, "efpol_ring: model %s is not provided (sl_equal only)\n", model);
+        return 193;
+    }
+    if (dbl != 0) {
+        fprintf(stderr, "efpol_ring: hierarchical doubling (DBLSTEP > 0) is not provided\n");
+        return 193;
+    }
+    if (interval < 1 || tmax < 1) {
+        fprintf(stderr, "efpol_ring: TIME and INTERVAL must be positive\n");
+        return 212;
+    }
+    int bl;
+    for (bl = 0; bl <= 9; bl++)
+        if ((1 << bl) >= lstart) break;
+    const int L = 1 << bl;
+
+    elp_job_spec spec;
+    elp_default_spec(&spec);
+    spec.L = L;
+    spec.N = nmono;
+    spec.density = density;
+    spec.seed = seed;
+    spec.steps_per_launch = interval < 100 ? (int)interval : 100;
+    elp_ctx* ctx = NULL;
+    elp_status st = elp_create(&spec, &ctx);
+    if (st) return die(st, 192);
+    elp_info info;
+    elp_get_info(ctx, &info);
+
+    char sub[4096], file[4200];
+    snprintf(sub, sizeof(sub), "%s/N_%d", dir, nmono);
+    if (mkdir_p(sub)) {
+        fprintf(stderr, "efpol_ring: cannot create %s\n", sub);
+        elp_destroy(ctx);
+        return 192;
+    }
+    if ((st = elp_init_melt(ctx))) return die(st, 192);
+    int32_t code = 0;
+    if ((st = elp_check(ctx, &code)) || code) {
+        elp_destroy(ctx);
+        return 192;
+    }
+    const double total = (double)tmax * nmono * info.P;
+    double done = 0;
+    for (long t = 0; t < tmax; t += interval) {
+        snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", sub, t);
+        if ((st = elp_write_tuv(ctx, file))) return die(st, 192);
+        double t0 = now_s();
+        if ((st = elp_run(ctx, interval)) || (st = elp_sync(ctx))) return die(st, 192);
+        double dt = now_s() - t0;
+        done += (double)interval * nmono * info.P;
+        printf("\b \b\b \b\rrun = 1/1, L=%d, [%.1lf%%] at %.2lf M/s", L, 100 * done / total,
+               1e-6 * interval * nmono * info.P / (dt > 0 ? dt : 1e-9));
+        fflush(NULL);
+    }
+    snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", sub, ((tmax - 1) / interval + 1) * interval);
+    if ((st = elp_write_tuv(ctx, file))) return die(st, 192);
+    if ((st = elp_check(ctx, &code)) || code) {
+        elp_destroy(ctx);
+        return 192;
+    }
+    /* WriteSimulationSettings, cpupol/efpol_io.c:111-140 */
+    snprintf(file, sizeof(file), "%s/simulation_settings.txt", sub);
+    FILE* f = fopen(file, "w");
+    if (!f) {
+        elp_destroy(ctx);
+        return 192;
+    }
+    fprintf(f, "Start_seed = %u\n", seed);
+    fprintf(f, "Length = %i\n", nmono);
+    fprintf(f, "Polytype = ring\n");
+    fprintf(f, "Density = %lf\n", density);
+    fprintf(f, "Latsize = %i\n", L);
+    fprintf(f, "Start_polysize = %i\n", nmono);
+    fprintf(f, "Double_step = %i\n", 0);
+    fprintf(f, "Interval = %li\n", interval);
+    fprintf(f, "Equilibrated = 0\n");
+    fprintf(f, "Npol = %i\n", info.P);
+    fprintf(f, "Polymodel = sl_equal\n");
+    fprintf(f, "Executable = efpol\n");
+    fclose(f);
+    elp_destroy(ctx);
+    printf("\nFinal sanity check succeeded\n");
+    return 0;
+}

@@ -1,0 +1,59 @@
+"""Drop-in front-ends: same arguments, directories, file names and exit
+codes as the reference programs, so do_run.sh and the analysis run on their
+output unchanged."""
+import gzip
+import os
+import subprocess
+
+import pytest
+
+import observables as obs
+from oracle_binding import Efpol
+
+pytestmark = pytest.mark.gpu
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(REPO, "mc-polymer-simulation_b200", "bin")
+GOLD = os.path.join(REPO, "tests", "golden")
+
+# keys and order of cpupol/efpol_io.c:111-140, as the reference's own run wrote them
+EFPOL_KEYS = ["Start_seed", "Length", "Polytype", "Density", "Latsize", "Start_polysize", "Double_step", "Interval",
+              "Equilibrated", "Npol", "Polymodel", "Executable"]
+
+
+def test_efpol_ring_cli(tmp_path):
+    out = tmp_path / "run"
+    r = subprocess.run([os.path.join(BIN, "efpol_ring"), "1", str(out), "1.2", "200", "100", "100", "0", "32",
+                        "sl_equal"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    d = out / "N_100"
+    assert sorted(os.listdir(d)) == ["simulation_settings.txt", "t=0_dev=0.res", "t=100_dev=0.res", "t=200_dev=0.res"]
+    ref0 = gzip.open(os.path.join(GOLD, "efpol_L32_N100_s1_t0.res.gz"), "rt").read()
+    assert (d / "t=0_dev=0.res").read_text() == ref0
+    for t in (100, 200):
+        L, start, bonds = obs.parse_tuv((d / f"t={t}_dev=0.res").read_text())
+        e = Efpol(32, 100, start.shape[0], 0)
+        assert e.read(obs.format_tuv(L, start, bonds)) == 0 and e.check() == 0
+    keys = [ln.split(" = ")[0] for ln in (d / "simulation_settings.txt").read_text().splitlines()]
+    assert keys == EFPOL_KEYS
+    assert "Npol = 393" in (d / "simulation_settings.txt").read_text()
+
+
+def test_efpol_ring_cli_rejects_unsupported(tmp_path):
+    r = subprocess.run([os.path.join(BIN, "efpol_ring"), "1", str(tmp_path), "1.2", "10", "5", "100", "0", "32",
+                        "sl_nonsense"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 193
+
+
+def test_gpupol_cli_resume_is_bit_identical(tmp_path):
+    exe = os.path.join(BIN, "gpupol3_cuda_ring")
+    a, b = tmp_path / "a", tmp_path / "b"
+    args = ["100", "{T}", "7", "{D}", "1.2", "0", "100", "32", "32", "32"]
+    run = lambda T, D: subprocess.run([exe] + [x.format(T=T, D=D) for x in args], capture_output=True, text=True,
+                                      timeout=120)
+    assert run(400, a).returncode == 0
+    assert run(200, b).returncode == 0
+    assert run(200, b).returncode == 0            # resumes from t=200 and runs 200 more
+    for t in (0, 100, 200, 300, 400):
+        assert (a / f"t={t}_dev=0.res").read_text() == (b / f"t={t}_dev=0.res").read_text(), t
+    s = (a / "simulation_settings.txt").read_text()
+    assert "Executable = efpol" in s and "Npol = 393" in s

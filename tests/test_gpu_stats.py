@@ -1,0 +1,80 @@
+"""Ensemble statistics of the GPU engine against the reference's CPU efpol.
+
+tests/golden/efpol_stats_*.json hold per-seed statistics of reference efpol
+runs (built from the reference sources, tests/golden/make_golden.py).  The
+GPU runs the same melts (same L, N, density, initial state, step count and
+dump interval) with other seeds -- its parallel schedule cannot reproduce
+efpol's random stream -- and the ensemble means must agree within the
+combined standard error of the two seed ensembles:
+
+    |mean_gpu - mean_ref| <= Z * sqrt(se_gpu^2 + se_ref^2),   Z = 4
+
+for the radius of gyration squared, the stored-length fraction, each of the
+first four bins of the run-length histogram, and the centre-of-mass MSD at
+each lag.  Whole-box domains (L = 16, 32) have no tile walls, so the time
+scale of the MSD is compared too.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import elp
+import observables as obs
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+Z = 4.0
+
+
+def gpu_ensemble(L, N, steps, interval, therm, lags, seeds):
+    b = elp.Batch([dict(L=L, N=N, seed=s, steps_per_launch=interval) for s in seeds])
+    b.init_melts()
+    nseed = len(seeds)
+    cms = [[] for _ in range(nseed)]
+    rg = [[] for _ in range(nseed)]
+    sl = [[] for _ in range(nseed)]
+    hist = [None] * nseed
+    for t in range(0, steps + 1, interval):
+        for j in range(nseed):
+            start, bonds = b.fetch(j)
+            start = start.astype(np.int64)
+            r, _, s = obs.chain_stats(start, bonds)
+            cms[j].append(obs.cms_tuv(start, bonds))
+            if t >= therm:
+                rg[j].append(r.mean())
+                sl[j].append(s.mean())
+                h = obs.run_length_hist(bonds)
+                hist[j] = h if hist[j] is None else hist[j] + h
+        if t < steps:
+            b.run(interval)
+    per = []
+    for j in range(nseed):
+        msd = obs.cms_msd(obs.unwrap_series(np.array(cms[j]), L)[therm // interval:], lags)
+        per.append(dict(rg2=float(np.mean(rg[j])), sl_frac=float(np.mean(sl[j])),
+                        run_hist=(hist[j] / hist[j].sum()).tolist(), msd=msd.tolist()))
+        assert b.check(j) == 0
+    return per
+
+
+def compare(ref, gpu, key, idx=None):
+    a = np.array([s[key] if idx is None else s[key][idx] for s in ref], dtype=float)
+    g = np.array([s[key] if idx is None else s[key][idx] for s in gpu], dtype=float)
+    se = np.sqrt(a.var(ddof=1) / len(a) + g.var(ddof=1) / len(g))
+    return abs(a.mean() - g.mean()), se, a.mean(), g.mean()
+
+
+@pytest.mark.parametrize("name,seeds", [("efpol_stats_L16_N50.json", range(2001, 2009)),
+                                        ("efpol_stats_L32_N100.json", range(3001, 3005))])
+def test_statistics_match_reference_efpol(name, seeds):
+    ref = json.load(open(os.path.join(GOLD, name)))
+    gpu = gpu_ensemble(ref["L"], ref["N"], ref["steps"], ref["interval"], ref["therm"], ref["msd_lags_intervals"],
+                       list(seeds))
+    rows = []
+    checks = [("rg2", None), ("sl_frac", None)] + [("run_hist", i) for i in range(4)] + \
+             [("msd", i) for i in range(len(ref["msd_lags_intervals"]))]
+    for key, idx in checks:
+        d, se, ma, mg = compare(ref["per_seed"], gpu, key, idx)
+        rows.append((key, idx, ma, mg, d, se))
+        assert d <= Z * se, f"{key}[{idx}]: efpol {ma:.5g} vs GPU {mg:.5g} differ by {d:.3g} > {Z} x {se:.3g}"
