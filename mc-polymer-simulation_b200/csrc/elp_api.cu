@@ -245,9 +245,9 @@ extern "C" elp_status elp_get_info(const elp_ctx* c, elp_info* info)
     info->tile[0] = c->g.tx; info->tile[1] = c->g.ty; info->tile[2] = c->g.tz;
     info->ncol = c->g.ncol;
     info->domains = c->domains;
-    info->threads = c->threads;
+    info->threads = c->G.threads;
     info->specialised = c->G.specialised;
-    info->smem_bytes = c->G.lay.bytes;
+    info->smem_bytes = c->G.smem;
     info->step = elp_group_step(&c->G, 0);
     info->device_bytes = c->device_bytes + c->wb.bytes;
     return ELP_OK;

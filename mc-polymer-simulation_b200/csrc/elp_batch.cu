@@ -344,9 +344,9 @@ extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info
     info->tile[0] = mm.g.tx; info->tile[1] = mm.g.ty; info->tile[2] = mm.g.tz;
     info->ncol = mm.g.ncol;
     info->domains = mm.g.periodic ? 1 : (mm.g.L / mm.g.tx) * (mm.g.L / mm.g.ty) * (mm.g.L / mm.g.tz);
-    info->threads = (G->lay.groups + 31) / 32 * 32;
+    info->threads = G->threads;
     info->specialised = G->specialised;
-    info->smem_bytes = G->lay.bytes;
+    info->smem_bytes = G->smem;
     info->step = elp_group_step(G, mm.index);
     info->device_bytes = b->device_bytes + b->wb.bytes;
     return ELP_OK;

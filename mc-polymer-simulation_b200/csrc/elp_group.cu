@@ -136,6 +136,14 @@ cudaError_t elp_group_commit(elp_group* G)
         return e;
     Sweep2Launch l = make_launch(G, G->g.periodic ? G->spl : 1, 0, 1);
     G->specialised = !G->generic && elp_launch_sweep2(&l, G->stream) == cudaSuccess;
+    if (G->specialised) {
+        G->threads = l.threads_out;
+        G->smem = l.smem_out;
+    } else {
+        G->threads = (G->lay.groups + 31) / 32 * 32;
+        G->threads = G->threads < 32 ? 32 : G->threads;
+        G->smem = G->lay.bytes;
+    }
     if (G->graph) {
         cudaGraphExecDestroy(G->graph);
         G->graph = nullptr;

@@ -19,6 +19,8 @@ struct elp_group {
     int nsm;
     int generic;                      // force the generic kernel
     int specialised;                  // a specialised kernel fits this group
+    int threads;                      // block size of the sweep kernel in use
+    size_t smem;                      // its dynamic shared memory per block
     int spl;                          // whole-box domains: steps per launch
     int use_graph;                    // tiled domains: replay launches from a CUDA graph
     int graph_steps;                  // launches captured per graph

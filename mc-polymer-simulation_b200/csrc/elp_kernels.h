@@ -58,6 +58,8 @@ struct Sweep2Launch {
     int check_only;                // only report whether a kernel fits
     double max_runs_per_domain;    // expected monomer-0 runs in one domain
     BatchLaunch args;
+    int threads_out;               // check_only: block size of the kernel that fits
+    size_t smem_out;               // check_only: its dynamic shared memory
 };
 
 extern "C" {

@@ -28,36 +28,51 @@ __device__ __forceinline__ void cp_async4(uint32_t* sdst, const uint32_t* gsrc)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP>
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K>
 struct Shape {
     static constexpr int R = TY * TZ;
-    static constexpr int A = R * (TX / NC);
-    static constexpr int G = A / 4;
+    static constexpr int A = R * (TX / NC);   // anchors per substep
+    static constexpr int G = A / 4;           // Philox counters per substep group
+    static constexpr int AT = A / K;          // threads that own anchors
     static constexpr int HALO = PER ? 0 : 2;
     static constexpr int OX = PER ? 0 : 1 + SX + SXY;
     static constexpr int WORDS = SXY * (TZ + HALO);
     static constexpr int SITES = TX * TY * TZ;
-    static constexpr size_t BYTES = (size_t)WORDS * 4 + 4096 + 27 * 16 * 4 + 64 * 4 + (size_t)CAP * 12 + 16;
+    // shared-memory word offsets: lattice, transition table (4096 bytes),
+    // neighbour offsets (27 x 16), colours, slot tables, slot count, and the
+    // Philox words of the current substep group when threads own < 4 anchors
+    static constexpr int TABW = WORDS;
+    static constexpr int OFFW = TABW + 1024;
+    static constexpr int COLW = OFFW + 27 * 16;
+    static constexpr int SCHW = COLW + 64;
+    static constexpr int SOFW = SCHW + CAP;
+    static constexpr int SSIW = SOFW + CAP;
+    static constexpr int NSLW = SSIW + CAP;
+    static constexpr int RNDW = (NSLW + 4) & ~3;
+    static constexpr int TOTW = RNDW + (K < 4 ? 4 * G : 0);
+    static constexpr size_t BYTES = (size_t)TOTW * 4;
 };
 
 constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
 
 extern __shared__ __align__(16) uint32_t g_smem[];
 
-// Four anchors of one thread, one substep.  Returns accepted moves.
+// The K anchors of one thread, one substep.  Returns accepted moves.
+// Anchor q takes its random byte at bit offset bsh[q] of the Philox word w.
 // Shared-memory word indices: lattice at 0, transition table (bytes) at
 // TABW words, neighbour offsets at OFFW words.
-template <bool PER, int NC, int TABW, int OFFW>
-__device__ __forceinline__ int substep4(uint32_t* slot_off, int* slot_site, const int (&base)[4], const int (&rot)[4],
-                                        const int (&clsyz)[4], const int (&xj)[4], int c, uint32_t w, int L)
+template <int K, bool PER, int NC, int TABW, int OFFW>
+__device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, const int (&base)[K], const int (&rot)[K],
+                                        const int (&clsyz)[K], const int (&xj)[K], const int (&bsh)[K], int c,
+                                        uint32_t w, int L)
 {
     uint32_t* S = g_smem;
     const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
     const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
-    int p[4], ob[4];
-    uint32_t wP[4], rb[4];
+    int p[K], ob[K];
+    uint32_t wP[K], rb[K];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < K; q++) {
         int xr = c + rot[q];
         xr -= xr >= NC ? NC : 0;
         p[q] = base[q] + xr;
@@ -68,23 +83,23 @@ __device__ __forceinline__ int substep4(uint32_t* slot_off, int* slot_site, cons
         }
         ob[q] = 16 * cls;
         wP[q] = S[p[q]];
-        rb[q] = (w >> (8 * q)) & 0xffu;
+        rb[q] = (w >> bsh[q]) & 0xffu;
     }
     // stage B: the next run (slot 1).  Loaded unconditionally: the index is
     // inside the anchor's radius-1 ball, which no other anchor of this
     // substep touches.
-    int pB[4];
-    uint32_t wB[4];
+    int pB[K];
+    uint32_t wB[K];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < K; q++) {
         pB[q] = p[q] + offs[ob[q] + (wP[q] & 15)];
         wB[q] = S[pB[q]];
     }
     // stage C: source bonds (b_{m-1}, b_m) and the table option.  Slot 0 needs
     // a run of at least two, slot 1 a next run inside the domain.
-    uint32_t e[4];
+    uint32_t e[K];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < K; q++) {
         const uint32_t s = rb[q] & 1, bo = wP[q] & 15;
         const bool live = wP[q] != 0 && (s ? wB[q] != ELP_WALL : wP[q] >= 2u * ELP_CUNIT);
         const uint32_t src2 = s ? ((wB[q] >= 2u * ELP_CUNIT) ? 0u : (wB[q] & 15)) : bo;
@@ -92,10 +107,10 @@ __device__ __forceinline__ int substep4(uint32_t* slot_off, int* slot_site, cons
         e[q] = tab[live ? idx : 0xFF0u];   // row (0xf, 0xf) holds only null moves
     }
     // stage D: target site P + dst1 (again inside the ball)
-    int pY[4];
-    uint32_t wY[4];
+    int pY[K];
+    uint32_t wY[K];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < K; q++) {
         pY[q] = p[q] + offs[ob[q] + (e[q] & 15)];
         wY[q] = S[pY[q]];
     }
@@ -103,7 +118,7 @@ __device__ __forceinline__ int substep4(uint32_t* slot_off, int* slot_site, cons
     // dst1 == 0 the target is P itself and P's store must come last.
     int acc = 0;
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < K; q++) {
         const uint32_t d1 = e[q] & 15, d2 = e[q] >> 4, s = rb[q] & 1;
         const bool join = d2 == 0;  // m joins the front of the next run
         const bool ok = e[q] && (join ? wY[q] != ELP_WALL : (d1 == 0 || wY[q] == 0));
@@ -144,22 +159,29 @@ __device__ __forceinline__ int substep4(uint32_t* slot_off, int* slot_site, cons
     return acc;
 }
 
-template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int THREADS, int MINB>
+// K anchors per thread: K = 4 keeps four independent moves in flight per
+// thread (instruction-level parallelism); K = 2 or 1 spreads a substep over
+// more warps (latency hiding when a domain has few anchors per SM).  The
+// random stream does not depend on K: anchor a = g + q * G always takes byte
+// q of Philox word (k & 3) of counter {t, d, k / 4, g}.
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 {
-    using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP>;
-    static_assert(SH::G <= THREADS, "threads");
+    using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K>;
+    static_assert(K == 1 || K == 2 || K == 4, "anchors per thread");
+    static_assert(SH::A % 4 == 0 && SH::AT <= THREADS, "threads");
     static_assert(CAP <= 2048, "slot numbers are 11 bits");
     static_assert((2 * NC) % 4 == 0, "substeps come in groups of four");
-    constexpr int TABW = SH::WORDS, OFFW = SH::WORDS + 1024;
+    constexpr int TABW = SH::TABW, OFFW = SH::OFFW;
     uint32_t* S = g_smem;
     uint8_t* tab = reinterpret_cast<uint8_t*>(g_smem + TABW);
-    int* offs = reinterpret_cast<int*>(tab + 4096);
-    uint32_t* col = reinterpret_cast<uint32_t*>(offs + 27 * 16);
-    uint32_t* slot_chain = col + 64;
-    uint32_t* slot_off = slot_chain + CAP;
-    int* slot_site = reinterpret_cast<int*>(slot_off + CAP);
-    uint32_t* nslots = reinterpret_cast<uint32_t*>(slot_site + CAP);
+    int* offs = reinterpret_cast<int*>(g_smem + OFFW);
+    uint32_t* col = g_smem + SH::COLW;
+    uint32_t* slot_chain = g_smem + SH::SCHW;
+    uint32_t* slot_off = g_smem + SH::SOFW;
+    int* slot_site = reinterpret_cast<int*>(g_smem + SH::SSIW);
+    uint32_t* nslots = g_smem + SH::NSLW;
+    uint4* rnd = reinterpret_cast<uint4*>(g_smem + SH::RNDW);
     const int tid = threadIdx.x;
     const int LP = TX;  // box edge of whole-box (periodic) domains
 
@@ -181,10 +203,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     if (!PER)
         for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = ELP_WALL;
 
-    int base[4], rot[4], clsyz[4], xj[4];
+    int base[K], rot[K], clsyz[K], xj[K], bsh[K];
+    const int gq = tid % SH::G;   // Philox counter word 3 of this thread's anchors
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        int an = tid + q * SH::G;
+    for (int q = 0; q < K; q++) {
+        int an = tid + q * SH::AT;
+        bsh[q] = 8 * (an / SH::G);
         int j = an / SH::R, row = an % SH::R;
         int y = row % TY, z = row / TY;
         int m = (2 * y + 3 * z) % NC;
@@ -195,7 +219,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         clsyz[q] = PER ? (3 * cy + 9 * cz) : 13;
         xj[q] = NC * j;
     }
-    const bool active = tid < SH::G;
+    const bool active = tid < SH::AT;
     const uint32_t step_dev = a.step_dev ? *a.step_dev : 0u;
 
     for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
@@ -237,7 +261,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 __syncthreads();
                 // monomer-0 runs: global chain id -> shared slot, run length inline.
                 // Few rings: find them through the chain records; many: scan the tile.
-                if (nchains * 4 <= SH::SITES) {
+                if (nchains <= THREADS) {
                     for (int ch = tid; ch < nchains; ch += THREADS) {
                         const uint4 r = *reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)ch);
                         const int gx = (int)(r.x % (uint32_t)L), gy = (int)((r.x / (uint32_t)L) % (uint32_t)L),
@@ -292,13 +316,21 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 #pragma unroll 1
             for (int k = 0; k < 2 * NC; k += 4) {
                 uint4 rw = make_uint4(0, 0, 0, 0);
-                if (active) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                if (K == 4) {
+                    if (active) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                } else {
+                    // G threads draw the group's words; the other reads of rnd
+                    // (previous group) are four barriers behind
+                    if (tid < SH::G) rnd[tid] = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                    __syncthreads();
+                    if (active) rw = rnd[gq];
+                }
                 const uint32_t rws[4] = {rw.x, rw.y, rw.z, rw.w};
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++) {
                     if (active)
-                        accepted += substep4<PER, NC, TABW, OFFW>(slot_off, slot_site, base, rot, clsyz, xj,
-                                                                  (int)col[k + kk], rws[kk], LP);
+                        accepted += substepK<K, PER, NC, TABW, OFFW>(slot_off, slot_site, base, rot, clsyz, xj, bsh,
+                                                                     (int)col[k + kk], rws[kk], LP);
                     __syncthreads();
                 }
             }
@@ -333,17 +365,22 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 }  // namespace elp
 
 // ---- dispatch ----------------------------------------------------------------
-template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int THREADS, int MINB>
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB>
 static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 {
-    using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP>;
-    auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, THREADS, MINB>;
+    using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K>;
+    auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, THREADS, MINB>;
     if (l->check_only) {
         // expected monomer-0 runs per domain must stay far inside the slot table
         const double m = l->max_runs_per_domain;
         if (!(PER ? m <= CAP : m + 8.0 * sqrt(m) + 16.0 <= CAP)) return cudaErrorNotSupported;
         // set the shared-memory limit here, outside any stream capture
-        return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
+        if (e == cudaSuccess) {
+            const_cast<Sweep2Launch*>(l)->threads_out = THREADS;
+            const_cast<Sweep2Launch*>(l)->smem_out = SH::BYTES;
+        }
+        return e;
     }
     int grid = l->args.nitems;
     if (grid > l->nsm * MINB) grid = l->nsm * MINB;
@@ -359,17 +396,19 @@ extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
 {
     const elp_geometry& g = l->geom;
     if (l->args.nsteps > 1 && !g.periodic) return cudaErrorNotSupported;
-#define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_)                                            \
+// shape: tile edges, whole box or tiled, colour modulus, shared-memory
+// strides, slot capacity, anchors per thread, threads, min blocks per SM
+#define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_)                                        \
     if (g.tx == X_ && g.ty == Y_ && g.tz == Z_ && g.periodic == PER_ && g.ncol == NC_ && l->sx == SX_ &&       \
         l->sxy == SXY_)                                                                                        \
-        return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, THR_, MINB_>(l, s);
-    SHAPE(32, 32, 32, 0, 16, 35, 1190, 2048, 512, 1)
-    SHAPE(32, 32, 16, 0, 16, 35, 1190, 1024, 256, 2)
-    SHAPE(16, 16, 16, 0, 16, 19, 342, 512, 64, 4)
-    SHAPE(48, 24, 24, 0, 16, 51, 1326, 2048, 448, 1)
-    SHAPE(16, 16, 16, 1, 16, 16, 256, 2048, 64, 1)
-    SHAPE(32, 32, 32, 1, 16, 33, 1056, 2048, 512, 1)
-    SHAPE(24, 24, 24, 1, 24, 24, 576, 2048, 160, 1)
+        return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_>(l, s);
+    SHAPE(32, 32, 32, 0, 16, 35, 1190, 2048, 2, 1024, 1)
+    SHAPE(32, 32, 16, 0, 16, 35, 1190, 1024, 1, 1024, 1)
+    SHAPE(16, 16, 16, 0, 16, 19, 342, 512, 1, 256, 4)
+    SHAPE(48, 24, 24, 0, 16, 51, 1326, 2048, 2, 864, 1)
+    SHAPE(16, 16, 16, 1, 16, 16, 256, 2048, 1, 256, 1)
+    SHAPE(32, 32, 32, 1, 16, 33, 1056, 2048, 2, 1024, 1)
+    SHAPE(24, 24, 24, 1, 24, 24, 576, 2048, 1, 576, 1)
 #undef SHAPE
     return cudaErrorNotSupported;
 }
