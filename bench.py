@@ -145,6 +145,30 @@ def cpu_baseline(w, steps, threads=1):
                       f"{moves:.3g} attempted moves in {wall:.2f} s"}
 
 
+def replica_seed(w, rank):
+    """Replica r of a workload runs the same melt with seed + r."""
+    return w["seed"] + rank
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    """Max of a host-side number over all ranks (the job's time is its
+    slowest replica's).  Replicas exchange nothing else; the reduction runs
+    on gloo over host memory."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_elp(args, rank, world):
     import torch
     import elp
@@ -155,15 +179,13 @@ def run_elp(args, rank, world):
     M = w["N"] * npol(w)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
-    m = elp.Melt(L=w["L"], N=w["N"], seed=w["seed"] + rank, device=dev)
+    m = elp.Melt(L=w["L"], N=w["N"], seed=replica_seed(w, rank), device=dev)
     m.init_melt()
     m.run(args.warmup)
     m.sync()
     info = m.info()
 
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    barrier(world)
     times = []
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
@@ -171,13 +193,8 @@ def run_elp(args, rank, world):
             torch.cuda.synchronize()
             times.append(m.run_timed(1))
     torch.cuda.synchronize()
-    total_ms = sum(times)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
+    total_ms = max_over_ranks(sum(times), world)
+    barrier(world)
     value = world * args.steps * M / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
     assert m.check() == 0, "integrity check failed after the timed run"
