@@ -134,6 +134,23 @@ elp_status elp_get_info(const elp_ctx* ctx, elp_info* info);
 elp_status elp_check_noalloc(const uint32_t* d_words, const uint32_t* d_records, int32_t L, int32_t N, int32_t P,
                              void* stream, int32_t* code);
 
+/* In-situ observables of the current state, computed on the device from the
+ * site words (no ring transfer).  Per ring, positions unwrapped along the
+ * ring from monomer 0's site as LoadPTL (analysis/mode_io.c:509-606) builds
+ * them from a TUV line:
+ *   cms_tuv[3*P]  mean (t, u, v) of the ring's monomers (ComputeTUVCMS-style
+ *                 lattice units; x = t+u-v, y = t-u, z = v, lengths / sqrt(2))
+ *   rg2[P]        radius of gyration squared in xyz / sqrt(2) units
+ *                 (ComputeGyration, analysis/mode_compute.c:191-203)
+ *   sl[P]         stored-length fraction: zero bonds / N (ComputeSL, :145-153)
+ *   run_hist[nbins] over the whole melt: bin k counts occupied sites holding
+ *                 k+1 monomers, the last bin those holding nbins or more
+ *                 (1 <= nbins <= ELP_OBS_MAX_BINS).
+ * Any output may be NULL.  Blocking.  The reference computes these offline
+ * from PTL files; there is no in-situ counterpart. */
+#define ELP_OBS_MAX_BINS 64
+elp_status elp_observe(elp_ctx* ctx, double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist, int32_t nbins);
+
 /* Raw state: words[L^3] site words, records[4*P]. Blocking. */
 elp_status elp_get_state(elp_ctx* ctx, uint32_t* words, uint32_t* records);
 elp_status elp_set_state(elp_ctx* ctx, const uint32_t* words, const uint32_t* records, uint64_t step);
@@ -151,6 +168,21 @@ elp_status elp_transition_table(uint8_t out[4096]);
  * with buf == NULL only the length is computed. */
 elp_status elp_format_tuv(int32_t L, int32_t N, int32_t P, const int32_t* start, const uint8_t* bonds,
                           char* buf, size_t cap, size_t* len);
+
+/* ---- PTL writer --------------------------------------------------------------
+ * Per-ring time series written while a run dumps: sample_dir/ptl/pol=<p>_dev=<dev>.res,
+ * the files the reference's create_ptl makes afterwards from the run's TUV
+ * dumps (analysis/create_ptl.c:46-115): "polId= p", "nTime= ntime", "len= N",
+ * then one "t u v <bond hex string>" line per dump.  Host only: needs no
+ * device.  Lines are buffered (buffer_bytes, 0 = 256 MiB) and appended to the
+ * files when the buffer fills and at close. */
+typedef struct elp_ptl elp_ptl;
+elp_status elp_ptl_open(const char* sample_dir, int32_t dev, int32_t P, int32_t N, int32_t ntime,
+                        size_t buffer_bytes, elp_ptl** out);
+/* One dump: start[3*P] (t,u,v of monomer 0), bonds[P*N]; ELP_ERR_STATE after ntime dumps. */
+elp_status elp_ptl_append(elp_ptl* w, const int32_t* start, const uint8_t* bonds);
+/* Flush and free; ELP_ERR_STATE if the number of dumps differs from ntime. */
+elp_status elp_ptl_close(elp_ptl* w);
 
 const char* elp_status_string(elp_status s);
 const char* elp_last_error(void);
@@ -178,6 +210,9 @@ elp_status elp_batch_run(elp_batch* b, int64_t nsteps);
 /* Same, timed with CUDA events across all group streams; blocks. */
 elp_status elp_batch_run_timed(elp_batch* b, int64_t nsteps, float* ms);
 elp_status elp_batch_sync(elp_batch* b);
+/* elp_observe for member j. */
+elp_status elp_batch_observe(elp_batch* b, int32_t j, double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist,
+                             int32_t nbins);
 elp_status elp_batch_fetch_chains(elp_batch* b, int32_t job, int32_t* start, uint8_t* bonds);
 elp_status elp_batch_get_state(elp_batch* b, int32_t job, uint32_t* words, uint32_t* records);
 elp_status elp_batch_check(elp_batch* b, int32_t job, int32_t* code);

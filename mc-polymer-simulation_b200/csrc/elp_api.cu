@@ -226,6 +226,18 @@ extern "C" elp_status elp_fetch_chains(elp_ctx* c, int32_t* start, uint8_t* bond
     return elp_fetch_rings(c->d_lat, c->d_rec, c->g.L, c->N, c->P, &c->wb, start, bonds, c->stream);
 }
 
+extern "C" elp_status elp_observe(elp_ctx* c, double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist,
+                                  int32_t nbins)
+{
+    if (!c) return elp_fail(ELP_ERR_ARG, "null argument");
+    if (!c->loaded) return elp_fail(ELP_ERR_STATE, "no configuration loaded");
+    ELP_CUDA_TRY(cudaSetDevice(c->device));
+    elp_status st = elp_device_errors(error_flags(c), c->stream);
+    if (st) return st;
+    return elp_observe_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, &c->wb, cms_tuv, rg2, sl, run_hist, nbins,
+                            c->stream);
+}
+
 extern "C" elp_status elp_check(elp_ctx* c, int32_t* code)
 {
     if (!c || !code) return elp_fail(ELP_ERR_ARG, "null argument");

@@ -292,6 +292,18 @@ extern "C" elp_status elp_batch_fetch_chains(elp_batch* b, int32_t j, int32_t* s
     return elp_fetch_rings(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, start, bonds, b->streams[(size_t)mm.group]);
 }
 
+extern "C" elp_status elp_batch_observe(elp_batch* b, int32_t j, double* cms_tuv, double* rg2, double* sl,
+                                        uint64_t* run_hist, int32_t nbins)
+{
+    elp_status st = job_ok(b, j);
+    if (st) return st;
+    const Member& mm = b->m[(size_t)j];
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
+    if ((st = errors_of(b, mm.group))) return st;
+    return elp_observe_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, cms_tuv, rg2, sl, run_hist, nbins,
+                            b->streams[(size_t)mm.group]);
+}
+
 extern "C" elp_status elp_batch_get_state(elp_batch* b, int32_t j, uint32_t* words, uint32_t* records)
 {
     elp_status st = job_ok(b, j);

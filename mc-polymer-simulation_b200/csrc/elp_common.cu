@@ -118,6 +118,7 @@ elp_status elp_device_errors(const uint32_t* d_flags, cudaStream_t s)
 void elp_walk_bufs_free(elp_walk_bufs* b)
 {
     cudaFree(b->d_start); cudaFree(b->d_bonds); cudaFree(b->d_status); cudaFree(b->d_visit); cudaFree(b->d_cnt);
+    cudaFree(b->d_obs);
     *b = elp_walk_bufs();
 }
 

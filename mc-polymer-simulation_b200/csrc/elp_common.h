@@ -33,7 +33,8 @@ struct elp_walk_bufs {
     int32_t* d_status = nullptr;
     uint32_t* d_visit = nullptr;
     unsigned long long* d_cnt = nullptr;
-    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0;
+    unsigned long long* d_obs = nullptr;   // observables: [P][6] ring sums + histogram
+    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0, cap_obs = 0;
     size_t bytes = 0;
 };
 void elp_walk_bufs_free(elp_walk_bufs* b);
@@ -41,6 +42,9 @@ void elp_walk_bufs_free(elp_walk_bufs* b);
 // Rebuild rings (start[3P], bonds[P*N]) of one melt into host buffers.
 elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
                            int32_t* start, uint8_t* bonds, cudaStream_t s);
+// Observables of one melt (elp_observe); any output may be null.
+elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+                            double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist, int nbins, cudaStream_t s);
 // Integrity check of one melt (code 0, 3 or 4 as CheckIntegrity).
 elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
                           int32_t* code, cudaStream_t s);

@@ -11,7 +11,8 @@
  * power of two (efpol.c:53-58) and the ring count is GetNPol.  Exit codes as
  * efpol: 0 ok, 192 integrity failure, 193 unknown/unsupported model.
  * Supported: MODEL sl_equal and DBLSTEP 0 (hierarchical doubling is not
- * provided).  "Executable = efpol" is written because the dynamics are
+ * provided).  With ELP_PTL=1 in the environment the per-ring time series
+ * DIR/N_<N>/ptl/pol=<p>_dev=0.res are written during the run as well.  "Executable = efpol" is written because the dynamics are
  * efpol's single-monomer dynamics (same move table and attempt rate).
  */
 #include <errno.h>
@@ -22,6 +23,7 @@
 #include <time.h>
 
 #include "elp.h"
+#include "elp_dump.h"
 
 static int mkdir_p(const char* path)
 {
@@ -121,11 +123,13 @@ int main(int argc, char** argv)
         elp_destroy(ctx);
         return 192;
     }
+    elp_dumper dumper;
+    if ((st = elp_dumper_open(&dumper, ctx, sub, (int32_t)((tmax - 1) / interval + 2)))) return die(st, 192);
     const double total = (double)tmax * nmono * info.P;
     double done = 0;
     for (long t = 0; t < tmax; t += interval) {
         snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", sub, t);
-        if ((st = elp_write_tuv(ctx, file))) return die(st, 192);
+        if ((st = elp_dumper_write(&dumper, ctx, file))) return die(st, 192);
         double t0 = now_s();
         if ((st = elp_run(ctx, interval)) || (st = elp_sync(ctx))) return die(st, 192);
         double dt = now_s() - t0;
@@ -135,7 +139,7 @@ int main(int argc, char** argv)
         fflush(NULL);
     }
     snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", sub, ((tmax - 1) / interval + 1) * interval);
-    if ((st = elp_write_tuv(ctx, file))) return die(st, 192);
+    if ((st = elp_dumper_write(&dumper, ctx, file))) return die(st, 192);
     if ((st = elp_check(ctx, &code)) || code) {
         elp_destroy(ctx);
         return 192;
@@ -160,6 +164,7 @@ int main(int argc, char** argv)
     fprintf(f, "Polymodel = sl_equal\n");
     fprintf(f, "Executable = efpol\n");
     fclose(f);
+    if ((st = elp_dumper_close(&dumper))) return die(st, 192);
     elp_destroy(ctx);
     printf("\nFinal sanity check succeeded\n");
     return 0;

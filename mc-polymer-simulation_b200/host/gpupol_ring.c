@@ -13,7 +13,10 @@
  * so it is bit-identical to an uninterrupted run.  The box must be cubic
  * (LT = LU = LV).  The initial melt is the efpol one and the dynamics are
  * efpol's single-monomer dynamics, hence "Executable = efpol" in the
- * settings (the analysis picks its time factor from that name).
+ * settings (the analysis picks its time factor from that name).  With
+ * ELP_PTL=1 in the environment a fresh run also writes the per-ring time
+ * series DIR/ptl/pol=<p>_dev=0.res during the run (not on resume: those files
+ * would have to cover the earlier dumps too).
  */
 #include <dirent.h>
 #include <errno.h>
@@ -24,6 +27,7 @@
 #include <time.h>
 
 #include "elp.h"
+#include "elp_dump.h"
 
 static int mkdir_p(const char* path)
 {
@@ -116,17 +120,21 @@ int main(int argc, char** argv)
     elp_info info;
     elp_get_info(ctx, &info);
     char file[4200];
+    elp_dumper dumper;
     long cur = newest_t(dir);
     if (cur >= 0) {
         printf("Starting from t=%ld\n", cur);
+        if (elp_ptl_requested()) fprintf(stderr, "gpupol3_cuda_ring: ELP_PTL is ignored when resuming\n");
+        memset(&dumper, 0, sizeof(dumper));
         snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", dir, cur);
         if ((st = elp_load_tuv(ctx, file, (uint64_t)cur))) return die(st);
         tmax += cur;
     } else {
         cur = 0;
         if ((st = elp_init_melt(ctx))) return die(st);
+        if ((st = elp_dumper_open(&dumper, ctx, dir, (int32_t)(1 + (tmax + interval - 1) / interval)))) return die(st);
         snprintf(file, sizeof(file), "%s/t=0_dev=0.res", dir);
-        if ((st = elp_write_tuv(ctx, file))) return die(st);
+        if ((st = elp_dumper_write(&dumper, ctx, file))) return die(st);
     }
     int32_t code = 0;
     if ((st = elp_check(ctx, &code)) || code) return code ? 192 : die(st);
@@ -139,7 +147,7 @@ int main(int argc, char** argv)
                dt, interval * (double)lt * lu * lv / (dt > 0 ? dt : 1e-9) / 1e6);
         fflush(stdout);
         snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", dir, cur + interval);
-        if ((st = elp_write_tuv(ctx, file))) return die(st);
+        if ((st = elp_dumper_write(&dumper, ctx, file))) return die(st);
     }
     printf("\nSimulation complete\n");
     if ((st = elp_check(ctx, &code)) || code) return code ? 192 : die(st);
@@ -162,6 +170,7 @@ int main(int argc, char** argv)
     fprintf(f, "FEQ_timestep = %i\n", fasteq);
     fprintf(f, "Release = elp-b200\n");
     fclose(f);
+    if ((st = elp_dumper_close(&dumper))) return die(st);
     elp_destroy(ctx);
     return 0;
 }

@@ -46,8 +46,11 @@ EXPORTED = [
     "elp_batch_run_timed", "elp_batch_sync", "elp_batch_fetch_chains", "elp_batch_get_state", "elp_batch_check",
     "elp_batch_accepted", "elp_batch_job_info", "elp_batch_destroy", "elp_autotune",
     "elp_server_default_opts", "elp_server_create", "elp_server_submit", "elp_server_poll", "elp_server_get_stats",
-    "elp_server_drain", "elp_server_destroy",
+    "elp_server_drain", "elp_server_destroy", "elp_check_noalloc", "elp_observe", "elp_batch_observe",
+    "elp_ptl_open", "elp_ptl_append", "elp_ptl_close",
 ]
+
+OBS_MAX_BINS = 64
 
 _lib = None
 
@@ -102,6 +105,12 @@ def lib():
         "elp_server_get_stats": (i32, [vp, vp]),
         "elp_server_drain": (i32, [vp, C.c_double]),
         "elp_server_destroy": (None, [vp]),
+        "elp_check_noalloc": (i32, [vp, vp, i32, i32, i32, vp, vp]),
+        "elp_observe": (i32, [vp, vp, vp, vp, vp, i32]),
+        "elp_batch_observe": (i32, [vp, i32, vp, vp, vp, vp, i32]),
+        "elp_ptl_open": (i32, [C.c_char_p, i32, i32, i32, i32, C.c_size_t, vp]),
+        "elp_ptl_append": (i32, [vp, vp, vp]),
+        "elp_ptl_close": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -142,6 +151,39 @@ def spec(L=32, N=100, P=0, density=1.2, seed=1, salt=0, periodic=-1, tile=(0, 0,
     s.tile[0], s.tile[1], s.tile[2] = tile
     s.ncol, s.device, s.steps_per_launch, s.kernel = ncol, device, steps_per_launch, kernel
     return s
+
+
+def _observe(call, P, nbins):
+    out = dict(cms_tuv=np.zeros((P, 3)), rg2=np.zeros(P), sl=np.zeros(P), run_hist=np.zeros(nbins, dtype=np.uint64))
+    check(call(out["cms_tuv"].ctypes.data, out["rg2"].ctypes.data, out["sl"].ctypes.data,
+               out["run_hist"].ctypes.data, nbins))
+    return out
+
+
+class PTLWriter:
+    """Per-ring time series files written during a run (elp_ptl_*): host only."""
+
+    def __init__(self, sample_dir, P, N, ntime, dev=0, buffer_bytes=0):
+        self.h = C.c_void_p()
+        self.P, self.N = P, N
+        check(lib().elp_ptl_open(sample_dir.encode(), dev, P, N, ntime, buffer_bytes, C.byref(self.h)))
+
+    def append(self, start, bonds):
+        start = np.ascontiguousarray(start, dtype=np.int32)
+        bonds = np.ascontiguousarray(bonds, dtype=np.uint8)
+        assert start.shape == (self.P, 3) and bonds.shape == (self.P, self.N)
+        check(lib().elp_ptl_append(self.h, start.ctypes.data, bonds.ctypes.data))
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            h, self.h = self.h, C.c_void_p()
+            check(lib().elp_ptl_close(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def autotune(copies=1, steps=20, **kw):
@@ -205,6 +247,10 @@ class Melt:
 
     def write_tuv(self, path):
         check(lib().elp_write_tuv(self.h, path.encode()))
+
+    def observe(self, nbins=16):
+        """In-situ observables (elp_observe): cms_tuv (P,3), rg2 (P), sl (P), run_hist (nbins)."""
+        return _observe(lambda *a: lib().elp_observe(self.h, *a), self.P, nbins)
 
     def check(self) -> int:
         code = C.c_int32()
@@ -287,6 +333,9 @@ class Batch:
         bonds = np.zeros((i.P, i.N), dtype=np.uint8)
         check(lib().elp_batch_fetch_chains(self.h, j, start.ctypes.data, bonds.ctypes.data))
         return start, bonds
+
+    def observe(self, j, nbins=16):
+        return _observe(lambda *a: lib().elp_batch_observe(self.h, j, *a), self.infos[j].P, nbins)
 
     def state(self, j):
         i = self.infos[j]

@@ -13,6 +13,9 @@ It compiles the reference's efpol from its own sources (oracle/Makefile target
   for the plain ring melt L=32, N=100, density 1.2, seed 1;
 * ``efpol_L16_N50_s3_t{0..100}.res.gz`` -- a short reference trajectory, one
   dump every 10 steps (pins the oracle's restatement step for step);
+* ``ptl_L16_N50_s3.json.gz`` -- the per-ring time series files that the
+  reference's create_ptl (analysis/create_ptl.c, built into oracle/_ref)
+  writes for that trajectory: {file name: content};
 * ``efpol_stats_L16_N50.json`` / ``efpol_stats_L32_N100.json`` -- ensemble
   statistics of reference efpol runs (16 and 8 distinct seeds) computed with
   oracle/observables.py: Rg^2, stored-length fraction, run-length histogram and
@@ -66,9 +69,22 @@ def stats_of_run(d, tmax, interval, L, therm):
     return float(np.mean(rg)), float(np.mean(sl)), (hist / hist.sum()).tolist(), msd.tolist()
 
 
+def make_ptl(refdir, efpol, tmp):
+    """The reference's create_ptl on the reference's own L=16 trajectory."""
+    d = run_efpol(efpol, 3, 16, 50, 100, 10, os.path.join(tmp, "ptl_run"))
+    subprocess.run([os.path.join(refdir, "create_ptl"), d], check=True, stdout=subprocess.DEVNULL)
+    files = {}
+    for name in sorted(os.listdir(os.path.join(d, "ptl"))):
+        with open(os.path.join(d, "ptl", name)) as f:
+            files[name] = f.read()
+    with gzip.GzipFile(os.path.join(HERE, "ptl_L16_N50_s3.json.gz"), "wb", mtime=0) as g:
+        g.write(json.dumps(files, sort_keys=True).encode())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", choices=["all", "ptl"], default="all")
     args = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={args.ref}"], check=True,
                    stdout=subprocess.DEVNULL)
@@ -76,6 +92,9 @@ def main():
     efpol = os.path.join(refdir, "efpol_ring")
     tmp = tempfile.mkdtemp(prefix="elp_golden_")
     try:
+        if args.only == "ptl":
+            make_ptl(refdir, efpol, tmp)
+            return
         for name, code in MODELS.items():
             raw = os.path.join(tmp, f"tab_{name}.bin")
             subprocess.run([os.path.join(refdir, "ref_table_dump_ring"), str(code), "5", raw], check=True)
@@ -94,6 +113,7 @@ def main():
             with open(os.path.join(d, f"t={t}_dev=0.res"), "rb") as f, \
                     gzip.GzipFile(os.path.join(HERE, f"efpol_L16_N50_s3_t{t}.res.gz"), "wb", mtime=0) as g:
                 g.write(f.read())
+        make_ptl(refdir, efpol, tmp)
 
         # efpol's seeding drops bit 0 of every Tausworthe word (util/rng.h:13-20,
         # 26-31), so seeds 2k and 2k+1 give the same run: use odd seeds only.

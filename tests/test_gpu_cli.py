@@ -57,3 +57,36 @@ def test_gpupol_cli_resume_is_bit_identical(tmp_path):
         assert (a / f"t={t}_dev=0.res").read_text() == (b / f"t={t}_dev=0.res").read_text(), t
     s = (a / "simulation_settings.txt").read_text()
     assert "Executable = efpol" in s and "Npol = 393" in s
+
+
+def _ptl_from_tuv_files(d, times):
+    """The per-ring files the reference's create_ptl would build from the TUV
+    dumps in d (analysis/create_ptl.c:46-115), made by the writer the tests pin
+    to create_ptl's own output (test_ptl.py)."""
+    import elp
+    dumps = [obs.parse_tuv((d / f"t={t}_dev=0.res").read_text())[1:] for t in times]
+    P, N = dumps[0][1].shape
+    ref = d.parent / (d.name + "_ref")
+    w = elp.PTLWriter(str(ref), P, N, len(dumps))
+    for start, bonds in dumps:
+        w.append(start, bonds)
+    w.close()
+    return {n: (ref / "ptl" / n).read_text() for n in os.listdir(ref / "ptl")}
+
+
+@pytest.mark.parametrize("prog", ["efpol_ring", "gpupol3_cuda_ring"])
+def test_cli_writes_ptl_in_situ(tmp_path, prog):
+    out = tmp_path / "run"
+    env = dict(os.environ, ELP_PTL="1")
+    if prog == "efpol_ring":
+        cmd = [os.path.join(BIN, prog), "5", str(out), "1.2", "250", "50", "60", "0", "16", "sl_equal"]
+        d, times = out / "N_60", [0, 50, 100, 150, 200, 250]
+    else:
+        cmd = [os.path.join(BIN, prog), "60", "250", "5", str(out), "1.2", "0", "50", "16", "16", "16"]
+        d, times = out, [0, 50, 100, 150, 200, 250]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 0, r.stderr
+    got = {n: (d / "ptl" / n).read_text() for n in os.listdir(d / "ptl")}
+    assert got == _ptl_from_tuv_files(d, times)
+    # newer than the settings file: create_ptl's NeedsUpdatePath (util/file.c:3-33) skips the pass
+    assert os.stat(d / "ptl" / "pol=0_dev=0.res").st_mtime >= os.stat(d / "simulation_settings.txt").st_mtime
