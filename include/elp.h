@@ -94,8 +94,14 @@ elp_status elp_load_tuv(elp_ctx* ctx, const char* path, uint64_t step);
 elp_status elp_run(elp_ctx* ctx, int64_t nsteps);
 
 /* Same as elp_run, timed with CUDA events recorded on the context's stream
- * around the launches; blocks and returns the elapsed milliseconds. */
+ * around the launches; blocks and returns the elapsed milliseconds.  Work
+ * the caller queued on the stream before (elp_stream) runs ahead of the
+ * first event and is not timed. */
 elp_status elp_run_timed(elp_ctx* ctx, int64_t nsteps, float* ms);
+
+/* The context's cudaStream_t, for ordering the caller's own device work
+ * (copies, cache flushes) with the context's launches.  The context owns it. */
+void* elp_stream(elp_ctx* ctx);
 
 elp_status elp_sync(elp_ctx* ctx);
 

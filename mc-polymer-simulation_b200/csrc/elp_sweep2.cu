@@ -54,6 +54,12 @@ struct Shape {
 };
 
 constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
+// Halo word of tiled domains: run length 1, b_out 0xf.  A slot-1 move whose
+// next run lies in the halo then looks up row (b_out(P), 0xf) of the table,
+// which ring melts never use and the kernel clears in its shared-memory copy,
+// so the move is null without a separate test; a target in the halo is
+// neither empty nor a run of the ring, so it is rejected as well.
+constexpr uint32_t HWALL = ELP_CUNIT | 15u;
 
 extern __shared__ __align__(16) uint32_t g_smem[];
 
@@ -74,7 +80,8 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
 #pragma unroll
     for (int q = 0; q < K; q++) {
         int xr = c + rot[q];
-        xr -= xr >= NC ? NC : 0;
+        if ((NC & (NC - 1)) == 0) xr &= NC - 1;
+        else xr -= xr >= NC ? NC : 0;
         p[q] = base[q] + xr;
         int cls = clsyz[q];
         if (PER) {
@@ -95,16 +102,19 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         pB[q] = p[q] + offs[ob[q] + (wP[q] & 15)];
         wB[q] = S[pB[q]];
     }
-    // stage C: source bonds (b_{m-1}, b_m) and the table option.  Slot 0 needs
-    // a run of at least two, slot 1 a next run inside the domain.
+    // stage C: source bonds (b_{m-1}, b_m) and the table option.  Slot 0
+    // (last monomer of P's run) uses row (0, b_out(P)) when the run holds two
+    // or more, else row (0, 0); slot 1 (first monomer of the next run B) uses
+    // row (b_out(P), B's run length > 1 ? 0 : b_out(B)).  Rows (0, 0) and
+    // (x, 0xf) hold only null moves, which covers an empty P (b_out 0, so B
+    // is P itself), a run of one in slot 0 and a next run in the halo.
     uint32_t e[K];
 #pragma unroll
     for (int q = 0; q < K; q++) {
         const uint32_t s = rb[q] & 1, bo = wP[q] & 15;
-        const bool live = wP[q] != 0 && (s ? wB[q] != ELP_WALL : wP[q] >= 2u * ELP_CUNIT);
-        const uint32_t src2 = s ? ((wB[q] >= 2u * ELP_CUNIT) ? 0u : (wB[q] & 15)) : bo;
-        const uint32_t idx = ((s ? bo : 0u) << 8) | (src2 << 4) | ((rb[q] >> 1) & 15);
-        e[q] = tab[live ? idx : 0xFF0u];   // row (0xf, 0xf) holds only null moves
+        const bool c2 = (s ? wB[q] : wP[q]) >= 2u * ELP_CUNIT;
+        const uint32_t src2 = s ? (c2 ? 0u : (wB[q] & 15)) : (c2 ? bo : 0u);
+        e[q] = tab[((s ? bo : 0u) << 8) | (src2 << 4) | ((rb[q] >> 1) & 15)];
     }
     // stage D: target site P + dst1 (again inside the ball)
     int pY[K];
@@ -121,7 +131,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
     for (int q = 0; q < K; q++) {
         const uint32_t d1 = e[q] & 15, d2 = e[q] >> 4, s = rb[q] & 1;
         const bool join = d2 == 0;  // m joins the front of the next run
-        const bool ok = e[q] && (join ? wY[q] != ELP_WALL : (d1 == 0 || wY[q] == 0));
+        const bool ok = e[q] && (join ? wY[q] != HWALL : (d1 == 0 || wY[q] == 0));
         uint32_t nP = wP[q] & ~15u;
         nP = (s == 0) ? nP - ELP_CUNIT : (d1 ? nP : nP + ELP_CUNIT);
         nP |= d1 ? d1 : d2;
@@ -172,6 +182,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     static_assert(SH::A % 4 == 0 && SH::AT <= THREADS, "threads");
     static_assert(CAP <= 2048, "slot numbers are 11 bits");
     static_assert((2 * NC) % 4 == 0, "substeps come in groups of four");
+    static_assert(THREADS % TX == 0, "tile columns are split evenly over the threads");
     constexpr int TABW = SH::TABW, OFFW = SH::OFFW;
     uint32_t* S = g_smem;
     uint8_t* tab = reinterpret_cast<uint8_t*>(g_smem + TABW);
@@ -183,9 +194,15 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     uint32_t* nslots = g_smem + SH::NSLW;
     uint4* rnd = reinterpret_cast<uint4*>(g_smem + SH::RNDW);
     const int tid = threadIdx.x;
+    const int cx = tid % TX;  // the tile column this thread loads, scans and stores
     const int LP = TX;  // box edge of whole-box (periodic) domains
 
-    for (int i = tid; i < 1024; i += THREADS) reinterpret_cast<uint32_t*>(tab)[i] = a.table[i];
+    // table words: entries 4i .. 4i+3 of row i / 4 = (src1 << 4) | src2; rows
+    // with a 0xf source (chain ends, absent from rings) are cleared
+    for (int i = tid; i < 1024; i += THREADS) {
+        const int row = i >> 2;
+        reinterpret_cast<uint32_t*>(tab)[i] = ((row & 15) == 15 || (row >> 4) == 15) ? 0u : a.table[i];
+    }
     for (int i = tid; i < 27 * 16; i += THREADS) {
         int cls = i >> 4, b = i & 15;
         int dt = elp_bt(b), du = elp_bu(b), dv = elp_bv(b);
@@ -201,7 +218,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         offs[i] = dt + SX * du + SXY * dv;
     }
     if (!PER)
-        for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = ELP_WALL;
+        for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = HWALL;
 
     int base[K], rot[K], clsyz[K], xj[K], bsh[K];
     const int gq = tid % SH::G;   // Philox counter word 3 of this thread's anchors
@@ -250,12 +267,15 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             if (st == 0) {
                 __syncthreads();  // the previous item's stores have read shared memory
                 if (tid == 0) *nslots = 0;
-                for (int i = tid; i < SH::SITES; i += THREADS) {
-                    const int x = i % TX, r = i / TX, y = r % TY, z = r / TY;
-                    int gx = D.x0 + x; gx -= gx >= L ? L : 0;
-                    int gy = D.y0 + y; gy -= gy >= L ? L : 0;
-                    int gz = D.z0 + z; gz -= gz >= L ? L : 0;
-                    cp_async4(S + SH::OX + x + SX * y + SXY * z, lat + (uint32_t)(gx + L * (gy + L * gz)));
+                {
+                    // each thread owns one x column of the tile: rows r = y + TY z
+                    int gx = D.x0 + cx; gx -= gx >= L ? L : 0;
+                    for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
+                        const int y = r % TY, z = r / TY;
+                        int gy = D.y0 + y; gy -= gy >= L ? L : 0;
+                        int gz = D.z0 + z; gz -= gz >= L ? L : 0;
+                        cp_async4(S + SH::OX + cx + SX * y + SXY * z, lat + (uint32_t)(gx + L * (gy + L * gz)));
+                    }
                 }
                 cp_async_wait_all();
                 __syncthreads();
@@ -281,9 +301,9 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                         }
                     }
                 } else {
-                    for (int i = tid; i < SH::SITES; i += THREADS) {
-                        const int x = i % TX, r = i / TX, y = r % TY, z = r / TY;
-                        const int idx = SH::OX + x + SX * y + SXY * z;
+                    for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
+                        const int y = r % TY, z = r / TY;
+                        const int idx = SH::OX + cx + SX * y + SXY * z;
                         const uint32_t wv = S[idx];
                         if (wv & ELP_LBIT) {
                             const uint32_t slot = atomicAdd(nslots, 1u);
@@ -346,12 +366,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 S[idx] = (wv & 15) | ELP_LBIT | (chain << 5);
             }
             __syncthreads();
-            for (int i = tid; i < SH::SITES; i += THREADS) {
-                const int x = i % TX, r = i / TX, y = r % TY, z = r / TY;
-                int gx = D.x0 + x; gx -= gx >= L ? L : 0;
+            int gx = D.x0 + cx; gx -= gx >= L ? L : 0;
+            for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
+                const int y = r % TY, z = r / TY;
                 int gy = D.y0 + y; gy -= gy >= L ? L : 0;
                 int gz = D.z0 + z; gz -= gz >= L ? L : 0;
-                lat[(uint32_t)(gx + L * (gy + L * gz))] = S[SH::OX + x + SX * y + SXY * z];
+                lat[(uint32_t)(gx + L * (gy + L * gz))] = S[SH::OX + cx + SX * y + SXY * z];
             }
         }
         if (J.acc) {

@@ -39,7 +39,7 @@ class Info(C.Structure):
 
 EXPORTED = [
     "elp_default_spec", "elp_create", "elp_init_melt", "elp_load_chains", "elp_load_tuv", "elp_run",
-    "elp_run_timed", "elp_sync", "elp_fetch_chains", "elp_write_tuv", "elp_check", "elp_get_info",
+    "elp_run_timed", "elp_stream", "elp_sync", "elp_fetch_chains", "elp_write_tuv", "elp_check", "elp_get_info",
     "elp_get_state", "elp_set_state", "elp_accepted", "elp_destroy", "elp_transition_table",
     "elp_format_tuv", "elp_status_string", "elp_last_error",
     "elp_batch_create", "elp_batch_size", "elp_batch_init_melts", "elp_batch_load_chains", "elp_batch_run",
@@ -71,6 +71,7 @@ def lib():
         "elp_load_tuv": (i32, [vp, C.c_char_p, u64]),
         "elp_run": (i32, [vp, i64]),
         "elp_run_timed": (i32, [vp, i64, vp]),
+        "elp_stream": (vp, [vp]),
         "elp_sync": (i32, [vp]),
         "elp_fetch_chains": (i32, [vp, vp, vp]),
         "elp_write_tuv": (i32, [vp, C.c_char_p]),
@@ -238,6 +239,10 @@ class Melt:
 
     def sync(self):
         check(lib().elp_sync(self.h))
+
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this melt (e.g. for torch.cuda.ExternalStream)."""
+        return lib().elp_stream(self.h) or 0
 
     def fetch(self):
         start = np.zeros((self.P, 3), dtype=np.int32)
