@@ -175,6 +175,25 @@ elp_status elp_transition_table(uint8_t out[4096]);
 elp_status elp_format_tuv(int32_t L, int32_t N, int32_t P, const int32_t* start, const uint8_t* bonds,
                           char* buf, size_t cap, size_t* len);
 
+/* Hierarchical doubling of a ring melt (efpol's DoubleLattice,
+ * cpupol/efpol_init.c:114-207): box 2L, rings of 8N, same P.  start_out[3*P]
+ * and bonds_out[P*8*N] receive the doubled rings.  Host only.  ELP_ERR_STATE
+ * if a two-site ring finds no free sites for its rebuilt form. */
+elp_status elp_double_chains(int32_t L, int32_t N, int32_t P, const int32_t* start, const uint8_t* bonds,
+                             int32_t* start_out, uint8_t* bonds_out);
+
+/* Upscaling of a ring melt's TUV file for the reference's GPU doubling runs
+ * (analysis/scaleup.c, called by do_run.sh): box 2L, rings 8x longer, each
+ * occupied site replaced by a seven-bond path through a 2x2x2 cube, with
+ * the reference's fixed random stream, so the output file is the
+ * reference's byte for byte.  Host only. */
+elp_status elp_scaleup_tuv(const char* in_path, const char* out_path);
+
+/* Ring pol_id of a TUV file as xyz text, one "x y z" line per monomer
+ * walked from the origin (analysis/tuv2xyz.c).  Host only.  ELP_ERR_ARG if
+ * pol_id is out of range. */
+elp_status elp_tuv_to_xyz(const char* in_path, int32_t pol_id, const char* out_path);
+
 /* ---- PTL writer --------------------------------------------------------------
  * Per-ring time series written while a run dumps: sample_dir/ptl/pol=<p>_dev=<dev>.res,
  * the files the reference's create_ptl makes afterwards from the run's TUV

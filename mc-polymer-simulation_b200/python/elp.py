@@ -47,7 +47,7 @@ EXPORTED = [
     "elp_batch_accepted", "elp_batch_job_info", "elp_batch_destroy", "elp_autotune",
     "elp_server_default_opts", "elp_server_create", "elp_server_submit", "elp_server_poll", "elp_server_get_stats",
     "elp_server_drain", "elp_server_destroy", "elp_check_noalloc", "elp_observe", "elp_batch_observe",
-    "elp_ptl_open", "elp_ptl_append", "elp_ptl_close",
+    "elp_ptl_open", "elp_ptl_append", "elp_ptl_close", "elp_double_chains",
 ]
 
 OBS_MAX_BINS = 64
@@ -112,6 +112,7 @@ def lib():
         "elp_ptl_open": (i32, [C.c_char_p, i32, i32, i32, i32, C.c_size_t, vp]),
         "elp_ptl_append": (i32, [vp, vp, vp]),
         "elp_ptl_close": (i32, [vp]),
+        "elp_double_chains": (i32, [i32, i32, i32, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -159,6 +160,17 @@ def _observe(call, P, nbins):
     check(call(out["cms_tuv"].ctypes.data, out["rg2"].ctypes.data, out["sl"].ctypes.data,
                out["run_hist"].ctypes.data, nbins))
     return out
+
+
+def double_chains(L, start, bonds):
+    """efpol's DoubleLattice on host chains: (2L, start', bonds' with 8N bonds per ring)."""
+    start = np.ascontiguousarray(start, dtype=np.int32)
+    bonds = np.ascontiguousarray(bonds, dtype=np.uint8)
+    P, N = bonds.shape
+    s2 = np.zeros((P, 3), dtype=np.int32)
+    b2 = np.zeros((P, 8 * N), dtype=np.uint8)
+    check(lib().elp_double_chains(L, N, P, start.ctypes.data, bonds.ctypes.data, s2.ctypes.data, b2.ctypes.data))
+    return 2 * L, s2, b2
 
 
 class PTLWriter:

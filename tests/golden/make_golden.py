@@ -16,6 +16,16 @@ It compiles the reference's efpol from its own sources (oracle/Makefile target
 * ``ptl_L16_N50_s3.json.gz`` -- the per-ring time series files that the
   reference's create_ptl (analysis/create_ptl.c, built into oracle/_ref)
   writes for that trajectory: {file name: content};
+* ``efpol_dbl_s5_t{1,100}_{in,out}.res.gz`` -- hierarchical doubling: the
+  reference efpol run with DBLSTEP=1 (final L=32, N=400; first level L=16,
+  N=50) for 1 and for 100 steps; ``in`` is its last dump of the first level,
+  ``out`` its first dump of the doubled level (DoubleLattice,
+  cpupol/efpol_init.c:114-207).  After one step many rings still sit on two
+  sites, which exercises the rebuilt-ring branch;
+* ``scaleup_<input>.res.gz`` -- the reference's analysis/scaleup.c output
+  for three of the TUV files above (compact t=0 rings and relaxed melts);
+  ``xyz_efpol_L16_N50_s3_t100_p{0,3,97}.txt.gz`` -- its analysis/tuv2xyz.c
+  export of three rings;
 * ``efpol_stats_L16_N50.json`` / ``efpol_stats_L32_N100.json`` -- ensemble
   statistics of reference efpol runs (16 and 8 distinct seeds) computed with
   oracle/observables.py: Rg^2, stored-length fraction, run-length histogram and
@@ -81,10 +91,42 @@ def make_ptl(refdir, efpol, tmp):
         g.write(json.dumps(files, sort_keys=True).encode())
 
 
+def make_double(efpol, tmp):
+    """Reference runs with one doubling step: last dump of level 0, first of level 1."""
+    for tmax in (1, 100):
+        out = os.path.join(tmp, f"dbl_{tmax}")
+        subprocess.run([efpol, "5", out, "1.2", str(tmax), str(tmax), "400", "1", "32", "sl_equal"], check=True,
+                       stdout=subprocess.DEVNULL)
+        for src, name in ((os.path.join(out, "N_50", f"t={tmax}_dev=0.res"), f"efpol_dbl_s5_t{tmax}_in.res.gz"),
+                          (os.path.join(out, "N_400", "t=0_dev=0.res"), f"efpol_dbl_s5_t{tmax}_out.res.gz")):
+            with open(src, "rb") as f, gzip.GzipFile(os.path.join(HERE, name), "wb", mtime=0) as g:
+                g.write(f.read())
+
+
+def make_export(refdir, tmp):
+    """The reference's scaleup and tuv2xyz on committed reference TUV files."""
+    for name in ("efpol_L16_N50_s3_t100", "efpol_L32_N100_s1_t0", "efpol_L32_N100_s1_t200"):
+        src = os.path.join(tmp, name + ".res")
+        with gzip.open(os.path.join(HERE, name + ".res.gz"), "rb") as f, open(src, "wb") as g:
+            g.write(f.read())
+        dst = os.path.join(tmp, "scaleup_" + name + ".res")
+        subprocess.run([os.path.join(refdir, "scaleup"), src, dst], check=True, stdout=subprocess.DEVNULL)
+        with open(dst, "rb") as f, gzip.GzipFile(os.path.join(HERE, "scaleup_" + name + ".res.gz"), "wb",
+                                                  mtime=0) as g:
+            g.write(f.read())
+    src = os.path.join(tmp, "efpol_L16_N50_s3_t100.res")
+    for pid in (0, 3, 97):
+        dst = os.path.join(tmp, f"xyz_{pid}.txt")
+        subprocess.run([os.path.join(refdir, "tuv2xyz"), src, dst, str(pid)], check=True, stdout=subprocess.DEVNULL)
+        with open(dst, "rb") as f, gzip.GzipFile(
+                os.path.join(HERE, f"xyz_efpol_L16_N50_s3_t100_p{pid}.txt.gz"), "wb", mtime=0) as g:
+            g.write(f.read())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["all", "ptl"], default="all")
+    ap.add_argument("--only", choices=["all", "ptl", "double", "export"], default="all")
     args = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={args.ref}"], check=True,
                    stdout=subprocess.DEVNULL)
@@ -94,6 +136,12 @@ def main():
     try:
         if args.only == "ptl":
             make_ptl(refdir, efpol, tmp)
+            return
+        if args.only == "double":
+            make_double(efpol, tmp)
+            return
+        if args.only == "export":
+            make_export(refdir, tmp)
             return
         for name, code in MODELS.items():
             raw = os.path.join(tmp, f"tab_{name}.bin")
@@ -114,6 +162,8 @@ def main():
                     gzip.GzipFile(os.path.join(HERE, f"efpol_L16_N50_s3_t{t}.res.gz"), "wb", mtime=0) as g:
                 g.write(f.read())
         make_ptl(refdir, efpol, tmp)
+        make_double(efpol, tmp)
+        make_export(refdir, tmp)
 
         # efpol's seeding drops bit 0 of every Tausworthe word (util/rng.h:13-20,
         # 26-31), so seeds 2k and 2k+1 give the same run: use odd seeds only.

@@ -90,3 +90,51 @@ def test_cli_writes_ptl_in_situ(tmp_path, prog):
     assert got == _ptl_from_tuv_files(d, times)
     # newer than the settings file: create_ptl's NeedsUpdatePath (util/file.c:3-33) skips the pass
     assert os.stat(d / "ptl" / "pol=0_dev=0.res").st_mtime >= os.stat(d / "simulation_settings.txt").st_mtime
+
+
+def test_efpol_ring_cli_doubling(tmp_path):
+    """DBLSTEP=1: L=16, N=50 for TIME steps, DoubleLattice, then L=32, N=400
+    (cpupol/efpol.c:84-101): both levels' dumps and settings, and the second
+    level starting from the doubled last state of the first."""
+    import elp
+    out = tmp_path / "run"
+    r = subprocess.run([os.path.join(BIN, "efpol_ring"), "9", str(out), "1.2", "100", "50", "400", "1", "32",
+                        "sl_equal"], capture_output=True, text=True, timeout=180)
+    assert r.returncode == 0, r.stderr
+    for n, L in ((50, 16), (400, 32)):
+        d = out / f"N_{n}"
+        assert sorted(os.listdir(d)) == ["simulation_settings.txt", "t=0_dev=0.res", "t=100_dev=0.res",
+                                         "t=50_dev=0.res"]
+        for t in (0, 50, 100):
+            Lf, start, bonds = obs.parse_tuv((d / f"t={t}_dev=0.res").read_text())
+            assert Lf == L and bonds.shape == (98, n)
+            e = Efpol(L, n, 98, 0)
+            assert e.read(obs.format_tuv(Lf, start, bonds)) == 0 and e.check() == 0
+        s = (d / "simulation_settings.txt").read_text()
+        assert f"Length = {n}\n" in s and f"Latsize = {L}\n" in s and "Start_polysize = 50\n" in s
+        assert f"Double_step = {0 if n == 50 else 1}\n" in s and "Npol = 98\n" in s
+    L, start, bonds = obs.parse_tuv((out / "N_50" / "t=100_dev=0.res").read_text())
+    L2, s2, b2 = elp.double_chains(L, start, bonds)
+    assert (out / "N_400" / "t=0_dev=0.res").read_text() == elp.format_tuv(L2, s2, b2)
+
+
+def test_gpupol_doubling_flow_with_scaleup(tmp_path):
+    """do_run.sh's GPU doubling (do_run.sh:290-330): run, scaleup the last
+    dump into a new directory as t=0, run there with 8N in a box of 2L."""
+    exe = os.path.join(BIN, "gpupol3_cuda_ring")
+    a, b = tmp_path / "a", tmp_path / "b"
+    r = subprocess.run([exe, "50", "100", "3", str(a), "1.2", "0", "50", "16", "16", "16"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    b.mkdir()
+    assert subprocess.run([os.path.join(BIN, "scaleup"), str(a / "t=100_dev=0.res"), str(b / "t=0_dev=0.res")],
+                          timeout=60).returncode == 0
+    r = subprocess.run([exe, "400", "100", "3", str(b), "1.2", "0", "50", "32", "32", "32"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert sorted(x for x in os.listdir(b) if x.startswith("t=")) == ["t=0_dev=0.res", "t=100_dev=0.res",
+                                                                      "t=50_dev=0.res"]
+    L, start, bonds = obs.parse_tuv((b / "t=100_dev=0.res").read_text())
+    assert L == 32 and bonds.shape == (98, 400)
+    e = Efpol(32, 400, 98, 0)
+    assert e.read(obs.format_tuv(L, start, bonds)) == 0 and e.check() == 0
