@@ -57,6 +57,9 @@ typedef struct elp_job_spec {
     int32_t device;           /* CUDA device ordinal */
     int32_t steps_per_launch; /* whole-box domains: steps per kernel launch (>=1) */
     int32_t kernel;           /* 0 auto (specialised when the shape has one), 1 generic */
+    int32_t linear;           /* 0 ring polymers (efpol_ring), 1 linear chains (efpol_lin): the last
+                               * bond of every chain is the end marker 0xf ('f' in TUV files).
+                               * Linear chains need a shape with a specialised kernel. */
 } elp_job_spec;
 
 typedef struct elp_info {
@@ -68,6 +71,7 @@ typedef struct elp_info {
     uint64_t smem_bytes;      /* dynamic shared memory per CTA */
     uint64_t step;            /* absolute steps done */
     uint64_t device_bytes;    /* device memory held by the context */
+    int32_t linear;           /* 1: linear chains */
 } elp_info;
 
 /* Fill a spec with defaults: density 1.2, auto geometry, device 0. */

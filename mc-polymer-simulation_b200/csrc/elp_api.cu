@@ -16,6 +16,7 @@
 struct elp_ctx {
     elp_geometry g;
     int N = 0, P = 0;
+    int linear = 0;
     uint32_t seed = 0, salt = 0;
     int device = 0;
     int nsm = 148;
@@ -55,6 +56,7 @@ extern "C" elp_status elp_create(const elp_job_spec* spec, elp_ctx** out)
     c->g = g;
     c->N = spec->N;
     c->P = P;
+    c->linear = spec->linear;
     c->seed = spec->seed;
     c->salt = spec->salt;
     c->device = spec->device;
@@ -95,11 +97,16 @@ extern "C" elp_status elp_create(const elp_job_spec* spec, elp_ctx** out)
                                         error_flags(c), c->stream);
         if (eg == cudaSuccess) {
             c->group_ready = 1;
-            elp_group_add(&c->G, c->d_lat, c->d_rec, c->d_acc, c->N, c->P, c->seed, c->salt, 0);
+            elp_group_add(&c->G, c->d_lat, c->d_rec, c->d_acc, c->N, c->P, c->seed, c->salt, 0, c->linear);
             eg = elp_group_commit(&c->G);
         }
         if (eg != cudaSuccess) {
             st = elp_fail(ELP_ERR_CUDA, "group set-up failed: %s", cudaGetErrorString(eg));
+            goto bad;
+        }
+        if (c->linear && !c->G.specialised) {
+            st = elp_fail(ELP_ERR_ARG, "linear chains need a domain shape with a specialised kernel (L=%d tile %dx%dx%d)",
+                          g.L, g.tx, g.ty, g.tz);
             goto bad;
         }
     }
@@ -141,7 +148,7 @@ extern "C" elp_status elp_load_chains(elp_ctx* c, const int32_t* start, const ui
     if (!c || !start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
     size_t S = (size_t)c->g.L * c->g.L * c->g.L;
     std::vector<uint32_t> lat(S), rec((size_t)c->P * ELP_REC_WORDS);
-    int rc = elp_chains_to_sites(c->g.L, c->N, c->P, start, bonds, lat.data(), rec.data());
+    int rc = elp_chains_to_sites(c->g.L, c->N, c->P, start, bonds, lat.data(), rec.data(), c->linear);
     if (rc == 3) return elp_fail(ELP_ERR_INTEGRITY, "two rings or two runs of a ring share a site (code 3)");
     if (rc) return elp_fail(ELP_ERR_INTEGRITY, "invalid ring: bad bond, not closed, or on a single site (code 4)");
     return upload(c, lat.data(), rec.data(), step);
@@ -152,7 +159,7 @@ extern "C" elp_status elp_init_melt(elp_ctx* c)
     if (!c) return elp_fail(ELP_ERR_ARG, "null context");
     std::vector<int32_t> start((size_t)c->P * 3);
     std::vector<uint8_t> bonds((size_t)c->P * c->N);
-    if (elp_initial_chains(c->g.L, c->N, c->P, start.data(), bonds.data()))
+    if (elp_initial_chains(c->g.L, c->N, c->P, start.data(), bonds.data(), c->linear))
         return elp_fail(ELP_ERR_ARG, "initial grid cannot hold %d rings of %d in L=%d", c->P, c->N, c->g.L);
     return elp_load_chains(c, start.data(), bonds.data(), 0);
 }
@@ -229,7 +236,7 @@ extern "C" elp_status elp_fetch_chains(elp_ctx* c, int32_t* start, uint8_t* bond
     ELP_CUDA_TRY(cudaSetDevice(c->device));
     elp_status st = elp_device_errors(error_flags(c), c->stream);
     if (st) return st;
-    return elp_fetch_rings(c->d_lat, c->d_rec, c->g.L, c->N, c->P, &c->wb, start, bonds, c->stream);
+    return elp_fetch_rings(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, start, bonds, c->stream);
 }
 
 extern "C" elp_status elp_observe(elp_ctx* c, double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist,
@@ -240,7 +247,7 @@ extern "C" elp_status elp_observe(elp_ctx* c, double* cms_tuv, double* rg2, doub
     ELP_CUDA_TRY(cudaSetDevice(c->device));
     elp_status st = elp_device_errors(error_flags(c), c->stream);
     if (st) return st;
-    return elp_observe_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, &c->wb, cms_tuv, rg2, sl, run_hist, nbins,
+    return elp_observe_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, cms_tuv, rg2, sl, run_hist, nbins,
                             c->stream);
 }
 
@@ -251,7 +258,7 @@ extern "C" elp_status elp_check(elp_ctx* c, int32_t* code)
     ELP_CUDA_TRY(cudaSetDevice(c->device));
     elp_status st = elp_device_errors(error_flags(c), c->stream);
     if (st) return st;
-    return elp_check_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, &c->wb, code, c->stream);
+    return elp_check_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, code, c->stream);
 }
 
 extern "C" elp_status elp_get_info(const elp_ctx* c, elp_info* info)
@@ -268,6 +275,7 @@ extern "C" elp_status elp_get_info(const elp_ctx* c, elp_info* info)
     info->smem_bytes = c->G.smem;
     info->step = elp_group_step(&c->G, 0);
     info->device_bytes = c->device_bytes + c->wb.bytes;
+    info->linear = c->linear;
     return ELP_OK;
 }
 

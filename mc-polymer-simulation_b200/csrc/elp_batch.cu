@@ -26,6 +26,7 @@ struct Member {
     int group, index;          // group and position inside it
     elp_geometry g;
     int N, P;
+    int linear;                // 1: linear chains
     uint32_t seed, salt;
     uint32_t* lat;
     uint32_t* rec;
@@ -99,6 +100,7 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
             return elp_fail(st, "melt %d: %s", j, elp_last_error());
         }
         mm.N = specs[j].N;
+        mm.linear = specs[j].linear;
         mm.seed = specs[j].seed;
         mm.salt = specs[j].salt;
         const int spl = mm.g.periodic ? (specs[j].steps_per_launch > 0 ? specs[j].steps_per_launch : 1) : 1;
@@ -166,7 +168,7 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
         ro += (size_t)mm.P * ELP_REC_WORDS;
         elp_group* G = b->groups[(size_t)mm.group];
         mm.index = (int)G->jobs.size();
-        elp_group_add(G, mm.lat, mm.rec, mm.acc, mm.N, mm.P, mm.seed, mm.salt, 0);
+        elp_group_add(G, mm.lat, mm.rec, mm.acc, mm.N, mm.P, mm.seed, mm.salt, 0, mm.linear);
     }
     for (elp_group* G : b->groups) {
         if ((e = elp_group_commit(G)) != cudaSuccess) {
@@ -174,6 +176,13 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
             return elp_fail(ELP_ERR_CUDA, "group commit failed: %s", cudaGetErrorString(e));
         }
     }
+    for (size_t j = 0; j < b->m.size(); j++)
+        if (b->m[j].linear && !b->groups[(size_t)b->m[j].group]->specialised) {
+            const elp_geometry gj = b->m[j].g;
+            elp_batch_destroy(b);
+            return elp_fail(ELP_ERR_ARG, "melt %zu: linear chains need a domain shape with a specialised kernel "
+                                         "(L=%d tile %dx%dx%d)", j, gj.L, gj.tx, gj.ty, gj.tz);
+        }
     *out = b;
     return ELP_OK;
 }
@@ -201,7 +210,7 @@ extern "C" elp_status elp_batch_load_chains(elp_batch* b, int32_t j, const int32
     Member& mm = b->m[(size_t)j];
     const size_t S = (size_t)mm.g.L * mm.g.L * mm.g.L;
     std::vector<uint32_t> lat(S), rec((size_t)mm.P * ELP_REC_WORDS);
-    int rc = elp_chains_to_sites(mm.g.L, mm.N, mm.P, start, bonds, lat.data(), rec.data());
+    int rc = elp_chains_to_sites(mm.g.L, mm.N, mm.P, start, bonds, lat.data(), rec.data(), mm.linear);
     if (rc == 3) return elp_fail(ELP_ERR_INTEGRITY, "melt %d: two runs share a site (code 3)", j);
     if (rc) return elp_fail(ELP_ERR_INTEGRITY, "melt %d: invalid ring (code 4)", j);
     ELP_CUDA_TRY(cudaSetDevice(b->device));
@@ -221,7 +230,7 @@ extern "C" elp_status elp_batch_init_melts(elp_batch* b)
         const Member& mm = b->m[j];
         std::vector<int32_t> start((size_t)mm.P * 3);
         std::vector<uint8_t> bonds((size_t)mm.P * mm.N);
-        if (elp_initial_chains(mm.g.L, mm.N, mm.P, start.data(), bonds.data()))
+        if (elp_initial_chains(mm.g.L, mm.N, mm.P, start.data(), bonds.data(), mm.linear))
             return elp_fail(ELP_ERR_ARG, "melt %zu: initial grid cannot hold %d rings of %d in L=%d", j, mm.P, mm.N,
                             mm.g.L);
         elp_status st = elp_batch_load_chains(b, (int32_t)j, start.data(), bonds.data(), 0);
@@ -289,7 +298,7 @@ extern "C" elp_status elp_batch_fetch_chains(elp_batch* b, int32_t j, int32_t* s
     const Member& mm = b->m[(size_t)j];
     ELP_CUDA_TRY(cudaSetDevice(b->device));
     if ((st = errors_of(b, mm.group))) return st;
-    return elp_fetch_rings(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, start, bonds, b->streams[(size_t)mm.group]);
+    return elp_fetch_rings(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, mm.linear, &b->wb, start, bonds, b->streams[(size_t)mm.group]);
 }
 
 extern "C" elp_status elp_batch_observe(elp_batch* b, int32_t j, double* cms_tuv, double* rg2, double* sl,
@@ -300,7 +309,7 @@ extern "C" elp_status elp_batch_observe(elp_batch* b, int32_t j, double* cms_tuv
     const Member& mm = b->m[(size_t)j];
     ELP_CUDA_TRY(cudaSetDevice(b->device));
     if ((st = errors_of(b, mm.group))) return st;
-    return elp_observe_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, cms_tuv, rg2, sl, run_hist, nbins,
+    return elp_observe_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, mm.linear, &b->wb, cms_tuv, rg2, sl, run_hist, nbins,
                             b->streams[(size_t)mm.group]);
 }
 
@@ -325,7 +334,7 @@ extern "C" elp_status elp_batch_check(elp_batch* b, int32_t j, int32_t* code)
     const Member& mm = b->m[(size_t)j];
     ELP_CUDA_TRY(cudaSetDevice(b->device));
     if ((st = errors_of(b, mm.group))) return st;
-    return elp_check_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, &b->wb, code, b->streams[(size_t)mm.group]);
+    return elp_check_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, mm.linear, &b->wb, code, b->streams[(size_t)mm.group]);
 }
 
 extern "C" elp_status elp_batch_accepted(elp_batch* b, int32_t j, uint64_t* acc)
@@ -358,6 +367,7 @@ extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info
     info->domains = mm.g.periodic ? 1 : (mm.g.L / mm.g.tx) * (mm.g.L / mm.g.ty) * (mm.g.L / mm.g.tz);
     info->threads = G->threads;
     info->specialised = G->specialised;
+    info->linear = mm.linear;
     info->smem_bytes = G->smem;
     info->step = elp_group_step(G, mm.index);
     info->device_bytes = b->device_bytes + b->wb.bytes;

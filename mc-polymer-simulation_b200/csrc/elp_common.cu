@@ -89,6 +89,9 @@ elp_status elp_resolve_spec(const elp_job_spec* spec, int* P, elp_geometry* g)
 {
     if (!spec) return elp_fail(ELP_ERR_ARG, "null spec");
     if (spec->L < 5 || spec->L > 1024) return elp_fail(ELP_ERR_ARG, "box edge L=%d out of range [5,1024]", spec->L);
+    if (spec->linear != 0 && spec->linear != 1) return elp_fail(ELP_ERR_ARG, "linear must be 0 or 1");
+    if (spec->linear && spec->kernel == 1)
+        return elp_fail(ELP_ERR_ARG, "linear chains run on the specialised kernels only");
     if (spec->N < 3 || spec->N > ELP_MAX_N)
         return elp_fail(ELP_ERR_ARG, "ring length N=%d outside [3,%d]", spec->N, ELP_MAX_N);
     int p = spec->P > 0 ? spec->P : elp_get_npol(spec->density, spec->N, (long)spec->L * spec->L * spec->L);
@@ -150,14 +153,14 @@ static elp_status ensure(elp_walk_bufs* b, int P, int N, size_t sites)
     return ELP_OK;
 }
 
-elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                            int32_t* start, uint8_t* bonds, cudaStream_t s)
 {
     elp_status st = ensure(b, P, N, 0);
     if (st) return st;
     WalkArgs w;
     memset(&w, 0, sizeof(w));
-    w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P;
+    w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P; w.linear = linear;
     w.start = b->d_start; w.bonds = b->d_bonds; w.status = b->d_status;
     ELP_CUDA_TRY(elp_launch_walk(&w, s));
     std::vector<int32_t> status((size_t)P);
@@ -171,7 +174,7 @@ elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int 
     return ELP_OK;
 }
 
-elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                           int32_t* code, cudaStream_t s)
 {
     size_t S = (size_t)L * L * L;
@@ -181,7 +184,7 @@ elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N
     ELP_CUDA_TRY(cudaMemsetAsync(b->d_cnt, 0, 8 * sizeof(unsigned long long), s));
     WalkArgs w;
     memset(&w, 0, sizeof(w));
-    w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P;
+    w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P; w.linear = linear;
     w.status = b->d_status; w.visit = b->d_visit; w.counters = b->d_cnt;
     ELP_CUDA_TRY(elp_launch_walk(&w, s));
     ELP_CUDA_TRY(elp_launch_scan(&w, s));

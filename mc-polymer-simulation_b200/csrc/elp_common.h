@@ -40,13 +40,13 @@ struct elp_walk_bufs {
 void elp_walk_bufs_free(elp_walk_bufs* b);
 
 // Rebuild rings (start[3P], bonds[P*N]) of one melt into host buffers.
-elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                            int32_t* start, uint8_t* bonds, cudaStream_t s);
 // Observables of one melt (elp_observe); any output may be null.
-elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                             double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist, int nbins, cudaStream_t s);
 // Integrity check of one melt (code 0, 3 or 4 as CheckIntegrity).
-elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                           int32_t* code, cudaStream_t s);
 
 // Parse TUV text for a melt of box L, P rings of N.  Returns ELP_OK or

@@ -59,8 +59,10 @@ extern "C" elp_status elp_double_chains(int32_t L, int32_t N, int32_t P, const i
         const uint8_t* b = bonds + (size_t)p * N;
         uint8_t* bo = bonds_out + (size_t)p * N8;
         const int32_t* s = start + 3 * (size_t)p;
-        for (int m = 0; m < N; m++)
+        for (int m = 0; m < N; m++) {
             if (b[m] > 15) return elp_fail(ELP_ERR_ARG, "ring %d: bond code %d is not 4-bit", p, b[m]);
+            if (b[m] == 15) return elp_fail(ELP_ERR_ARG, "chain %d ends in 0xf: DoubleLattice doubles rings only", p);
+        }
         if (s[0] < 0 || s[0] >= L || s[1] < 0 || s[1] >= L || s[2] < 0 || s[2] >= L)
             return elp_fail(ELP_ERR_ARG, "ring %d: start outside the box", p);
         // the plain doubling, which also marks the doubled sites occupied

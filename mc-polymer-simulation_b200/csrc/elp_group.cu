@@ -94,10 +94,11 @@ cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int 
 }
 
 void elp_group_add(elp_group* G, uint32_t* lat, uint32_t* rec, unsigned long long* acc, int N, int nchains,
-                   uint32_t seed, uint32_t salt, uint64_t step)
+                   uint32_t seed, uint32_t salt, uint64_t step, int linear)
 {
     BatchJob j;
     memset(&j, 0, sizeof(j));
+    j.linear = linear;
     j.lat = lat;
     j.rec = rec;
     j.acc = acc;

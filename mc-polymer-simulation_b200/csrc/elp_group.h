@@ -45,7 +45,7 @@ struct elp_group {
 cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int generic, int spl,
                            const uint32_t* d_table, uint32_t* d_error, cudaStream_t stream);
 void elp_group_add(elp_group* G, uint32_t* lat, uint32_t* rec, unsigned long long* acc, int N, int nchains,
-                   uint32_t seed, uint32_t salt, uint64_t step);
+                   uint32_t seed, uint32_t salt, uint64_t step, int linear);
 // Upload the job table and work items; decide specialised vs generic.
 cudaError_t elp_group_commit(elp_group* G);
 // Set the absolute step of melt j (after loading a configuration).

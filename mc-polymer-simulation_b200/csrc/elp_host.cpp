@@ -202,7 +202,7 @@ int elp_get_npol(double density, int N, long sites)
 // CreatePolymers, cpupol/efpol_init.c:239-283: rings on a delta-spaced grid,
 // monomer 0 alone, bond +v, the other N-1 monomers stored on the next site,
 // closing bond -v.  Returns 0, or 1 if the grid cannot hold P rings.
-int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds)
+int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds, int linear)
 {
     if (N < 3 || P < 1) return 1;
     int delta;
@@ -220,7 +220,7 @@ int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds)
         uint8_t* b = bonds + (size_t)p * N;
         memset(b, 0, (size_t)N);
         b[0] = 0x4;
-        b[N - 1] = 0xb;
+        b[N - 1] = linear ? 0xf : 0xb;   // end marker, or the -v bond closing the ring
     }
     return 0;
 }
@@ -234,7 +234,8 @@ static inline uint32_t wrap_site(int L, long t, long u, long v)
     return (uint32_t)(t + (long)L * (u + (long)L * v));
 }
 
-int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t* bonds, uint32_t* lat, uint32_t* rec)
+int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t* bonds, uint32_t* lat, uint32_t* rec,
+                        int linear)
 {
     size_t S = (size_t)L * L * L;
     memset(lat, 0, S * sizeof(uint32_t));
@@ -244,13 +245,15 @@ int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t
         long t = start[3 * p], u = start[3 * p + 1], v = start[3 * p + 2];
         if (t < 0 || u < 0 || v < 0 || t >= L || u >= L || v >= L) return 4;
         int nz = 0;
+        if (linear && b[N - 1] != 0xf) return 4;
         for (int m = 0; m < N; m++) {
             pos[(size_t)m] = wrap_site(L, t, u, v);
-            if (b[m] && !elp_valid_bond(b[m])) return 4;
+            if (b[m] && !elp_valid_bond(b[m]) && !(linear && m == N - 1)) return 4;
             t += elp_bt(b[m]); u += elp_bu(b[m]); v += elp_bv(b[m]);
             nz += b[m] ? 1 : 0;
         }
-        if (wrap_site(L, t, u, v) != pos[0] || nz < 2) return 4;
+        // a ring closes on itself; a linear chain's runs end with the marker's run
+        if (!linear && (wrap_site(L, t, u, v) != pos[0] || nz < 2)) return 4;
         int first = 0;
         while (!b[(first + N - 1) % N]) first++;
         int m = first, done = 0;

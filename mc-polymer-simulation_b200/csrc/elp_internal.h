@@ -29,6 +29,7 @@
 // Philox counter layout (c2 high bits select the stream).
 #define ELP_STREAM_COLOUR 0x40000000u
 #define ELP_STREAM_SHIFT 0x80000000u
+#define ELP_STREAM_HEAD 0x20000000u    // monomer-0 moves of linear chains: ctr {t, d, k | HEAD, anchor}
 
 #ifdef __CUDACC__
 #define ELP_HD __host__ __device__ __forceinline__
@@ -69,7 +70,7 @@ void elp_philox_host(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[
 void elp_build_table(uint8_t tab[4096]);
 int elp_get_npol(double density, int N, long sites);
 // CreatePolymers-equivalent start layout (cpupol/efpol_init.c:239-283).
-int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds);
+int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds, int linear);
 // chains -> site words + records; returns 0, 3 (two runs on one site), 4 (bad chain)
 int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t* bonds, uint32_t* lat,
-                        uint32_t* rec);
+                        uint32_t* rec, int linear);

@@ -26,6 +26,7 @@ struct WalkArgs {
     int32_t* status;               // [P]
     uint32_t* visit;               // [L^3] visit counters or null
     unsigned long long* counters;  // [5]: runs walked, runs found, monomers found, bad sites, shared sites
+    int linear;                    // 1: chains end in a run with b_out 0xf instead of closing
 };
 
 // One melt of a batch as the specialised kernel sees it.
@@ -37,6 +38,7 @@ struct BatchJob {
     int ntx, nty, ntz;             // domains per axis
     uint32_t seed, salt;
     uint32_t step0;                // absolute step at step_base == 0
+    int linear;                    // 1: linear chains (head moves of monomer 0 at its anchor)
 };
 
 struct BatchLaunch {

@@ -5,7 +5,8 @@
 // taken relative to monomer 0's site and unwrapped along the ring:
 //   St, Su, Sv    sums of the lattice coordinates (t, u, v)
 //   Sq            sum of x^2 + y^2 + z^2 with x = t+u-v, y = t-u, z = v
-//   runs          occupied sites of the ring (zero bonds = N - runs)
+//   runs          occupied sites of the ring (zero bonds = N - runs; a
+//                 linear chain ends in the run whose b_out is the marker 0xf)
 // and a block-level histogram of run lengths (monomers per occupied site).
 // Only these P x 48 bytes go to the host, where the centre of mass, the
 // radius of gyration and the stored-length fraction are formed exactly as
@@ -25,7 +26,7 @@ namespace elp {
 struct ObsArgs {
     const uint32_t* lat;
     const uint32_t* rec;
-    int L, N, P, nbins;
+    int L, N, P, nbins, linear;
     unsigned long long* out;    // [P][6]: St, Su, Sv, Sq, runs | status << 32, site of monomer 0
     unsigned long long* hist;   // [nbins]
 };
@@ -41,7 +42,7 @@ __global__ void observe_kernel(ObsArgs a)
         const size_t S = (size_t)L * L * L;
         const uint32_t site = a.rec[ELP_REC_WORDS * p], cnt = a.rec[ELP_REC_WORDS * p + 1],
                        off = a.rec[ELP_REC_WORDS * p + 2];
-        int bad = (site >= S || off >= cnt || cnt == 0) ? 1 : 0;
+        int bad = (site >= S || off >= cnt || cnt == 0 || (a.linear && off != 0)) ? 1 : 0;
         if (!bad) {
             const uint32_t w = a.lat[site];
             if (!(w & ELP_LBIT) || (w >> 5) != (uint32_t)p) bad = 1;
@@ -53,7 +54,8 @@ __global__ void observe_kernel(ObsArgs a)
         uint32_t here = cnt - off, cur = site, len = cnt;
         while (!bad) {
             const uint32_t bo = a.lat[cur] & 15;
-            if (!elp_valid_bond(bo) || mono + (long)here > (long)N) { bad = 1; break; }
+            const bool end = a.linear && bo == 15;   // last run of a linear chain
+            if (!(elp_valid_bond(bo) || end) || mono + (long)here > (long)N) { bad = 1; break; }
             const long long x = dt + du - dv, y = dt - du, z = dv;
             st += (long long)here * dt;
             su += (long long)here * du;
@@ -62,6 +64,7 @@ __global__ void observe_kernel(ObsArgs a)
             mono += here;
             runs++;
             atomicAdd(&hist[(len < (uint32_t)a.nbins ? len : (uint32_t)a.nbins) - 1], 1ull);
+            if (end) break;
             // next run
             int t = (int)(cur % (uint32_t)L), u = (int)((cur / (uint32_t)L) % (uint32_t)L),
                 v = (int)(cur / ((uint32_t)L * L));
@@ -103,7 +106,7 @@ __global__ void observe_kernel(ObsArgs a)
 
 }  // namespace elp
 
-elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, elp_walk_bufs* b,
+elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                             double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist, int nbins, cudaStream_t s)
 {
     if (nbins < 0 || nbins > ELP_OBS_MAX_BINS)
@@ -118,7 +121,7 @@ elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int
         b->cap_obs = need;
     }
     elp::ObsArgs a;
-    a.lat = lat; a.rec = rec; a.L = L; a.N = N; a.P = P;
+    a.lat = lat; a.rec = rec; a.L = L; a.N = N; a.P = P; a.linear = linear;
     a.nbins = nbins > 0 ? nbins : 1;
     a.out = b->d_obs;
     a.hist = b->d_obs + (size_t)P * 6;
@@ -149,7 +152,8 @@ elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int
             const __int128 num = (__int128)N * (__int128)r[3] - (sx * sx + sy * sy + sz * sz);
             rg2[p] = (double)num / (2.0 * n * n);
         }
-        if (sl) sl[p] = (double)((unsigned long long)N - (r[4] & 0xffffffffull)) / n;
+        // zero bonds over the chain's bonds (a linear chain's end marker is none)
+        if (sl) sl[p] = (double)((unsigned long long)N - (r[4] & 0xffffffffull)) / (linear ? n - 1.0 : n);
     }
     if (run_hist)
         for (int i = 0; i < nbins; i++) run_hist[i] = h[(size_t)i];

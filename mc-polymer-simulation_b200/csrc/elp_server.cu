@@ -239,8 +239,8 @@ static bool admit(elp_server* s)
         std::vector<int32_t> start((size_t)j->P * 3);
         std::vector<uint8_t> bonds((size_t)j->P * j->spec.N);
         std::vector<uint32_t> lat(S), rec((size_t)j->P * ELP_REC_WORDS);
-        if (elp_initial_chains(j->g.L, j->spec.N, j->P, start.data(), bonds.data()) ||
-            elp_chains_to_sites(j->g.L, j->spec.N, j->P, start.data(), bonds.data(), lat.data(), rec.data())) {
+        if (elp_initial_chains(j->g.L, j->spec.N, j->P, start.data(), bonds.data(), 0) ||
+            elp_chains_to_sites(j->g.L, j->spec.N, j->P, start.data(), bonds.data(), lat.data(), rec.data(), 0)) {
             cudaFreeAsync(j->lat, gp->s);
             cudaFreeAsync(j->rec, gp->s);
             fail_job(s, j, ELP_ERR_ARG, "initial melt does not fit the box");
@@ -272,7 +272,7 @@ static bool rebuild(elp_server* s, SGroup* gp)
         SJob* j = gp->members[i];
         j->index = (int)i;
         elp_group_add(&G, j->lat, j->rec, s->d_acc, j->spec.N, j->P, j->spec.seed, j->spec.salt,
-                      (uint64_t)j->done_steps);
+                      (uint64_t)j->done_steps, 0);
     }
     gp->dirty = false;
     if (gp->members.empty()) return true;
@@ -289,11 +289,11 @@ static bool drain_snap(elp_server* s, Snap& sn)
     w->final = sn.final;
     w->start.resize((size_t)j->P * 3);
     w->bonds.resize((size_t)j->P * j->spec.N);
-    elp_status st = elp_fetch_rings(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, &s->wb, w->start.data(),
+    elp_status st = elp_fetch_rings(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, 0, &s->wb, w->start.data(),
                                     w->bonds.data(), s->side);
     if (sn.final && st == ELP_OK) {
         int32_t code = -1;
-        if (elp_check_melt(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, &s->wb, &code, s->side) == ELP_OK)
+        if (elp_check_melt(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, 0, &s->wb, &code, s->side) == ELP_OK)
             j->integrity = code;
     }
     cudaFreeAsync(sn.d_lat, s->side);
@@ -486,6 +486,7 @@ extern "C" elp_status elp_server_submit(elp_server* s, const elp_job_spec* spec,
 {
     if (!s || !spec) return elp_fail(ELP_ERR_ARG, "null argument");
     if (nsteps < 1) return elp_fail(ELP_ERR_ARG, "a job needs at least one step");
+    if (spec->linear) return elp_fail(ELP_ERR_ARG, "the server runs ring melts; run linear chains with elp_create");
     const int64_t Q = s->o.quantum;
     if (nsteps % Q) return elp_fail(ELP_ERR_ARG, "steps must be a multiple of the quantum (%lld)", (long long)Q);
     if (dump_interval < 0 || (dump_interval && dump_interval % Q))

@@ -48,18 +48,19 @@ struct Shape {
     static constexpr int SOFW = SCHW + CAP;
     static constexpr int SSIW = SOFW + CAP;
     static constexpr int NSLW = SSIW + CAP;
-    static constexpr int RNDW = (NSLW + 4) & ~3;
+    static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
+    static constexpr int RNDW = (HTABW + 64 + 4) & ~3;
     static constexpr int TOTW = RNDW + (K < 4 ? 4 * G : 0);
     static constexpr size_t BYTES = (size_t)TOTW * 4;
 };
 
 constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
-// Halo word of tiled domains: run length 1, b_out 0xf.  A slot-1 move whose
-// next run lies in the halo then looks up row (b_out(P), 0xf) of the table,
-// which ring melts never use and the kernel clears in its shared-memory copy,
-// so the move is null without a separate test; a target in the halo is
-// neither empty nor a run of the ring, so it is rejected as well.
-constexpr uint32_t HWALL = ELP_CUNIT | 15u;
+// Halo word of tiled domains: run length 1, b_out 3 (not a bond).  A slot-1
+// move whose next run lies in the halo then looks up row (b_out(P), 3) of
+// the table, which the kernel clears in its shared-memory copy, so the move
+// is null without a separate test; a target in the halo is neither empty nor
+// a run of the chain, so it is rejected as well.
+constexpr uint32_t HWALL = ELP_CUNIT | 3u;
 
 extern __shared__ __align__(16) uint32_t g_smem[];
 
@@ -67,10 +68,11 @@ extern __shared__ __align__(16) uint32_t g_smem[];
 // Anchor q takes its random byte at bit offset bsh[q] of the Philox word w.
 // Shared-memory word indices: lattice at 0, transition table (bytes) at
 // TABW words, neighbour offsets at OFFW words.
-template <int K, bool PER, int NC, int TABW, int OFFW>
+template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW>
 __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, const int (&base)[K], const int (&rot)[K],
-                                        const int (&clsyz)[K], const int (&xj)[K], const int (&bsh)[K], int c,
-                                        uint32_t w, int L)
+                                        const int (&clsyz)[K], const int (&xj)[K], const int (&bsh)[K],
+                                        const int (&an)[K], int c, uint32_t w, int L, bool lin, uint32_t t, int d,
+                                        int k, uint2 key)
 {
     uint32_t* S = g_smem;
     const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
@@ -164,7 +166,45 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         if (ok && s) S[pB[q]] = nB;
         if (ok && d1) S[pY[q]] = nY;
         if (ok) S[p[q]] = nP;
+        wP[q] = ok ? nP : wP[q];
         acc += ok ? 1 : 0;
+    }
+    // linear chains: monomer 0 has no predecessor and moves about monomer 1,
+    // tried at the anchor holding it after that anchor's regular attempt:
+    // with probability 1/2 (bit 0 of its own Philox word) one option of row
+    // (0xf, run length > 1 ? 0 : b_out) -- it leaves to the empty site P - u
+    // (its bond to monomer 1 becoming u), or, alone on P, joins the next run
+    if (lin) {
+        const uint8_t* htab = reinterpret_cast<const uint8_t*>(g_smem + HTABW);
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            const uint32_t w0 = wP[q];
+            if (!(w0 & ELP_LBIT)) continue;
+            const uint4 h = philox(make_uint4(t, (uint32_t)d, (uint32_t)k | ELP_STREAM_HEAD, (uint32_t)an[q]), key);
+            if (!(h.x & 1)) continue;
+            const uint32_t cP = w0 >> ELP_CSHIFT, bo = w0 & 15;
+            const uint32_t e = htab[((cP >= 2 ? 0u : bo) << 4) | ((h.x >> 1) & 15)];
+            if (!e) continue;
+            const uint32_t d2 = e >> 4, slot = (w0 >> 5) & 0x7FFu;
+            if (cP >= 2) {
+                const int pY = p[q] + offs[ob[q] + ((~d2) & 15u)];
+                if (S[pY] == 0) {
+                    S[pY] = d2 | (w0 & LMASK) | ELP_CUNIT;
+                    S[p[q]] = (w0 & ~LMASK) - ELP_CUNIT;
+                    slot_site[slot] = pY;
+                    acc++;
+                }
+            } else {
+                const int pB = p[q] + offs[ob[q] + bo];
+                const uint32_t wB = S[pB];
+                if (wB != HWALL) {
+                    S[pB] = (wB + ELP_CUNIT) | (w0 & LMASK);
+                    S[p[q]] = 0;
+                    slot_site[slot] = pB;
+                    acc++;
+                }
+            }
+        }
     }
     return acc;
 }
@@ -183,7 +223,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     static_assert(CAP <= 2048, "slot numbers are 11 bits");
     static_assert((2 * NC) % 4 == 0, "substeps come in groups of four");
     static_assert(THREADS % TX == 0, "tile columns are split evenly over the threads");
-    constexpr int TABW = SH::TABW, OFFW = SH::OFFW;
+    constexpr int TABW = SH::TABW, OFFW = SH::OFFW, HTABW = SH::HTABW;
     uint32_t* S = g_smem;
     uint8_t* tab = reinterpret_cast<uint8_t*>(g_smem + TABW);
     int* offs = reinterpret_cast<int*>(g_smem + OFFW);
@@ -197,12 +237,16 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     const int cx = tid % TX;  // the tile column this thread loads, scans and stores
     const int LP = TX;  // box edge of whole-box (periodic) domains
 
-    // table words: entries 4i .. 4i+3 of row i / 4 = (src1 << 4) | src2; rows
-    // with a 0xf source (chain ends, absent from rings) are cleared
+    // table words: entries 4i .. 4i+3 of row i / 4 = (src1 << 4) | src2.
+    // Cleared: rows with a source that is no bond (3, 12: halo words) and
+    // rows with src1 = 0xf (slot 1 at the last run of a linear chain, which
+    // has no next run); rows (0xf, x) are kept apart for monomer-0 moves.
     for (int i = tid; i < 1024; i += THREADS) {
-        const int row = i >> 2;
-        reinterpret_cast<uint32_t*>(tab)[i] = ((row & 15) == 15 || (row >> 4) == 15) ? 0u : a.table[i];
+        const int s1 = i >> 6, s2 = (i >> 2) & 15;
+        const bool nobond = s1 == 3 || s1 == 12 || s1 == 15 || s2 == 3 || s2 == 12;
+        reinterpret_cast<uint32_t*>(tab)[i] = nobond ? 0u : a.table[i];
     }
+    for (int i = tid; i < 64; i += THREADS) g_smem[HTABW + i] = a.table[960 + i];
     for (int i = tid; i < 27 * 16; i += THREADS) {
         int cls = i >> 4, b = i & 15;
         int dt = elp_bt(b), du = elp_bu(b), dv = elp_bv(b);
@@ -220,11 +264,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     if (!PER)
         for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = HWALL;
 
-    int base[K], rot[K], clsyz[K], xj[K], bsh[K];
+    int base[K], rot[K], clsyz[K], xj[K], bsh[K], anq[K];
     const int gq = tid % SH::G;   // Philox counter word 3 of this thread's anchors
 #pragma unroll
     for (int q = 0; q < K; q++) {
         int an = tid + q * SH::AT;
+        anq[q] = an;
         bsh[q] = 8 * (an / SH::G);
         int j = an / SH::R, row = an % SH::R;
         int y = row % TY, z = row / TY;
@@ -248,6 +293,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         uint32_t* rec = J.rec;
         const int nchains = J.nchains;
         const uint2 key = make_uint2(J.seed, J.salt);
+        const bool lin = J.linear != 0;
         const int ntx = J.ntx, nty = J.nty;
         Dom D;
         D.S = S; D.tab = tab; D.rec = rec;
@@ -349,8 +395,9 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++) {
                     if (active)
-                        accepted += substepK<K, PER, NC, TABW, OFFW>(slot_off, slot_site, base, rot, clsyz, xj, bsh,
-                                                                     (int)col[k + kk], rws[kk], LP);
+                        accepted += substepK<K, PER, NC, TABW, OFFW, HTABW>(
+                            slot_off, slot_site, base, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d,
+                            k + kk, key);
                     __syncthreads();
                 }
             }

@@ -6,8 +6,10 @@
 // GetAllRingPolymers / UpdatePolymerWithLabels (gpupol2/oclpol.c:183-376).
 // With visit counters it also proves the integrity conditions of the
 // reference's CheckIntegrity (cpupol/efpol_io.c:158-211): every ring closes
-// after exactly N monomers through valid bonds, and (with scan_kernel) every
-// occupied site belongs to exactly one ring and the monomer total is N*P.
+// after exactly N monomers through valid bonds (a linear chain instead ends
+// after exactly N monomers in a run whose b_out is the marker 0xf, with
+// monomer 0 first in its run), and (with scan_kernel) every occupied site
+// belongs to exactly one chain and the monomer total is N*P.
 #include <cuda_runtime.h>
 
 #include "elp_internal.h"
@@ -33,7 +35,7 @@ __global__ void walk_kernel(WalkArgs a)
     const size_t S = (size_t)L * L * L;
     uint32_t site = a.rec[ELP_REC_WORDS * p], cnt = a.rec[ELP_REC_WORDS * p + 1], off = a.rec[ELP_REC_WORDS * p + 2];
     int bad = 0;
-    if (site >= S || off >= cnt || cnt == 0) bad = 1;
+    if (site >= S || off >= cnt || cnt == 0 || (a.linear && off != 0)) bad = 1;
     uint32_t w = bad ? 0 : a.lat[site];
     if (!bad && (!(w & ELP_LBIT) || (w >> 5) != (uint32_t)p)) bad = 1;
     if (bad) { a.status[p] = 4; return; }
@@ -48,7 +50,8 @@ __global__ void walk_kernel(WalkArgs a)
     unsigned long long runs = 0;
     for (;;) {
         uint32_t bo = a.lat[cur] & 15;
-        if (!elp_valid_bond(bo) || i + (long)here > (long)N) { bad = 1; break; }
+        const bool end = a.linear && bo == 15;   // last run of a linear chain
+        if (!(elp_valid_bond(bo) || end) || i + (long)here > (long)N) { bad = 1; break; }
         if (b) {
             for (uint32_t k = 0; k + 1 < here; k++) b[i + k] = 0;
             b[i + here - 1] = (uint8_t)bo;
@@ -56,6 +59,7 @@ __global__ void walk_kernel(WalkArgs a)
         i += here;
         runs++;
         if (a.visit) atomicAdd(&a.visit[cur], 1u);
+        if (end) break;
         cur = step_site(cur, bo, L);
         uint32_t wn = a.lat[cur];
         if (!wn) { bad = 1; break; }
@@ -93,7 +97,7 @@ __global__ void scan_kernel(WalkArgs a)
             if (w & 0xFFE0u) badc++;   // bits 5-15 must be clear
         }
         mono += c;
-        if (!elp_valid_bond(w & 15) || c == 0 || (a.visit && v == 0)) badc++;
+        if (!(elp_valid_bond(w & 15) || (a.linear && (w & 15) == 15)) || c == 0 || (a.visit && v == 0)) badc++;
         if (a.visit && v > 1) multi++;
     }
     for (int o = 16; o > 0; o >>= 1) {

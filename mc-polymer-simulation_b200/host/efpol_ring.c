@@ -1,6 +1,7 @@
 /*
- * efpol_ring -- drop-in replacement of the reference's CPU program efpol_ring
- * (cpupol/efpol.c:4-114) running the ELP sweep on the GPU.
+ * efpol_ring / efpol_lin -- drop-in replacements of the reference's CPU
+ * programs efpol_ring and efpol_lin (cpupol/efpol.c:4-114 built for rings
+ * or linear chains) running the ELP sweep on the GPU.
  *
  *   efpol_ring SEED DIR DENSITY TIME INTERVAL NMONO DBLSTEP L MODEL
  *
@@ -29,6 +30,16 @@
 #include "elp.h"
 #include "elp_dump.h"
 
+/* Built twice: efpol_ring, and with ELP_LINEAR_CHAINS as efpol_lin, the
+ * reference's efpol built with POL_TYPE=POL_LIN (cpupol/Makefile:13-14). */
+#ifdef ELP_LINEAR_CHAINS
+#define PROG "efpol_lin"
+#define LINEAR 1
+#else
+#define PROG "efpol_ring"
+#define LINEAR 0
+#endif
+
 static int mkdir_p(const char* path)
 {
     char buf[4096];
@@ -55,7 +66,7 @@ static double now_s(void)
 
 static int die(elp_status st, int code)
 {
-    fprintf(stderr, "efpol_ring: %s: %s\n", elp_status_string(st), elp_last_error());
+    fprintf(stderr, PROG ": %s: %s\n", elp_status_string(st), elp_last_error());
     return code;
 }
 
@@ -85,11 +96,16 @@ int main(int argc, char** argv)
             printf("Unknown polymer model, aborting!\n");
             return 193;
         }
-        fprintf(stderr, "efpol_ring: model %s is not provided (sl_equal only)\n", model);
+        fprintf(stderr, PROG ": model %s is not provided (sl_equal only)\n", model);
+        return 193;
+    }
+    if (LINEAR && dbl != 0) {
+        /* DoubleLattice doubles rings only (linear chains would keep an end marker inside the chain) */
+        fprintf(stderr, PROG ": hierarchical doubling (DBLSTEP > 0) is provided for rings only\n");
         return 193;
     }
     if (dbl < 0 || dbl > 6) {
-        fprintf(stderr, "efpol_ring: DBLSTEP must be in [0, 6]\n");
+        fprintf(stderr, PROG ": DBLSTEP must be in [0, 6]\n");
         return 193;
     }
     for (int i = 0; i < dbl; i++) {
@@ -101,7 +117,7 @@ int main(int argc, char** argv)
         return 212;
     }
     if (interval < 1 || tmax < 1) {
-        fprintf(stderr, "efpol_ring: TIME and INTERVAL must be positive\n");
+        fprintf(stderr, PROG ": TIME and INTERVAL must be positive\n");
         return 212;
     }
     int bl;
@@ -113,7 +129,7 @@ int main(int argc, char** argv)
     for (int i = 0, n = nmono; i <= dbl; i++, n *= 8) {
         snprintf(sub, sizeof(sub), "%s/N_%d", dir, n);
         if (mkdir_p(sub)) {
-            fprintf(stderr, "efpol_ring: cannot create %s\n", sub);
+            fprintf(stderr, PROG ": cannot create %s\n", sub);
             return 192;
         }
     }
@@ -133,6 +149,7 @@ int main(int argc, char** argv)
         spec.seed = seed;
         spec.salt = (uint32_t)lev;
         spec.steps_per_launch = interval < 100 ? (int)interval : 100;
+        spec.linear = LINEAR;
         elp_ctx* ctx = NULL;
         elp_status st = elp_create(&spec, &ctx);
         if (st) return die(st, 192);
@@ -193,7 +210,7 @@ int main(int argc, char** argv)
         }
         fprintf(f, "Start_seed = %u\n", seed);
         fprintf(f, "Length = %i\n", N);
-        fprintf(f, "Polytype = ring\n");
+        fprintf(f, LINEAR ? "Polytype = lin\n" : "Polytype = ring\n");
         fprintf(f, "Density = %lf\n", density);
         fprintf(f, "Latsize = %i\n", L);
         fprintf(f, "Start_polysize = %i\n", nmono);

@@ -29,6 +29,16 @@
 #include "elp.h"
 #include "elp_dump.h"
 
+/* Built twice: gpupol3_cuda_ring, and with ELP_LINEAR_CHAINS as
+ * gpupol3_cuda_lin (do_run.sh:261-262 names the program after POL_TYPE). */
+#ifdef ELP_LINEAR_CHAINS
+#define PROG "gpupol3_cuda_lin"
+#define LINEAR 1
+#else
+#define PROG "gpupol3_cuda_ring"
+#define LINEAR 0
+#endif
+
 static int mkdir_p(const char* path)
 {
     char buf[4096];
@@ -71,7 +81,7 @@ static long newest_t(const char* dir)
 
 static int die(elp_status st)
 {
-    fprintf(stderr, "gpupol3_cuda_ring: %s: %s\n", elp_status_string(st), elp_last_error());
+    fprintf(stderr, PROG ": %s: %s\n", elp_status_string(st), elp_last_error());
     return 192;
 }
 
@@ -96,15 +106,15 @@ int main(int argc, char** argv)
     if (argc > 11) equil = atoi(argv[11]);
     if (argc > 12) dbl = atoi(argv[12]);
     if (lt != lu || lt != lv) {
-        fprintf(stderr, "gpupol3_cuda_ring: only cubic boxes are provided (got %dx%dx%d)\n", lt, lu, lv);
+        fprintf(stderr, PROG ": only cubic boxes are provided (got %dx%dx%d)\n", lt, lu, lv);
         return 192;
     }
     if (interval < 1 || tmax < 1) {
-        fprintf(stderr, "gpupol3_cuda_ring: TIME and INTERVAL must be positive\n");
+        fprintf(stderr, PROG ": TIME and INTERVAL must be positive\n");
         return 192;
     }
     if (mkdir_p(dir)) {
-        fprintf(stderr, "gpupol3_cuda_ring: cannot create %s\n", dir);
+        fprintf(stderr, PROG ": cannot create %s\n", dir);
         return 192;
     }
     elp_job_spec spec;
@@ -114,6 +124,7 @@ int main(int argc, char** argv)
     spec.density = density;
     spec.seed = seed;
     spec.steps_per_launch = interval < 100 ? (int)interval : 100;
+    spec.linear = LINEAR;
     elp_ctx* ctx = NULL;
     elp_status st = elp_create(&spec, &ctx);
     if (st) return die(st);
@@ -124,7 +135,7 @@ int main(int argc, char** argv)
     long cur = newest_t(dir);
     if (cur >= 0) {
         printf("Starting from t=%ld\n", cur);
-        if (elp_ptl_requested()) fprintf(stderr, "gpupol3_cuda_ring: ELP_PTL is ignored when resuming\n");
+        if (elp_ptl_requested()) fprintf(stderr, PROG ": ELP_PTL is ignored when resuming\n");
         memset(&dumper, 0, sizeof(dumper));
         snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", dir, cur);
         if ((st = elp_load_tuv(ctx, file, (uint64_t)cur))) return die(st);
@@ -156,7 +167,7 @@ int main(int argc, char** argv)
     if (!f) return 192;
     fprintf(f, "Start_seed = %u\n", seed);
     fprintf(f, "Length = %i\n", nmono);
-    fprintf(f, "Polytype = ring\n");
+    fprintf(f, LINEAR ? "Polytype = lin\n" : "Polytype = ring\n");
     fprintf(f, "Density = %lf\n", density);
     fprintf(f, "Latsize = %i\n", lt);
     fprintf(f, "Start_polysize = %i\n", nmono);

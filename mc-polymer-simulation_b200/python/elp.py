@@ -28,13 +28,14 @@ class JobSpec(C.Structure):
     _fields_ = [("L", C.c_int32), ("N", C.c_int32), ("P", C.c_int32), ("density", C.c_double),
                 ("seed", C.c_uint32), ("salt", C.c_uint32), ("periodic", C.c_int32), ("tile", C.c_int32 * 3),
                 ("ncol", C.c_int32), ("device", C.c_int32), ("steps_per_launch", C.c_int32),
-                ("kernel", C.c_int32)]
+                ("kernel", C.c_int32), ("linear", C.c_int32)]
 
 
 class Info(C.Structure):
     _fields_ = [("L", C.c_int32), ("N", C.c_int32), ("P", C.c_int32), ("periodic", C.c_int32),
                 ("tile", C.c_int32 * 3), ("ncol", C.c_int32), ("domains", C.c_int32), ("threads", C.c_int32),
-                ("specialised", C.c_int32), ("smem_bytes", C.c_uint64), ("step", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("specialised", C.c_int32), ("smem_bytes", C.c_uint64), ("step", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("linear", C.c_int32)]
 
 
 EXPORTED = [
@@ -145,13 +146,14 @@ def format_tuv(L, start, bonds) -> str:
 
 
 def spec(L=32, N=100, P=0, density=1.2, seed=1, salt=0, periodic=-1, tile=(0, 0, 0), ncol=0, device=0,
-         steps_per_launch=1, kernel=0) -> JobSpec:
+         steps_per_launch=1, kernel=0, linear=0) -> JobSpec:
     s = JobSpec()
     lib().elp_default_spec(C.byref(s))
     s.L, s.N, s.P, s.density, s.seed, s.salt = L, N, P, density, seed, salt
     s.periodic = periodic
     s.tile[0], s.tile[1], s.tile[2] = tile
     s.ncol, s.device, s.steps_per_launch, s.kernel = ncol, device, steps_per_launch, kernel
+    s.linear = 1 if linear else 0
     return s
 
 

@@ -82,12 +82,19 @@ def to_xyz(tuv: np.ndarray) -> np.ndarray:
     return np.stack([t + u - v, t - u, v], axis=-1).astype(np.float64) / np.sqrt(2.0)
 
 
+def is_linear(bonds: np.ndarray) -> bool:
+    """Linear chains end in the marker bond 0xf (TUV character 'f')."""
+    return bool(np.all(bonds[:, -1] == 0xF))
+
+
 def chain_stats(start: np.ndarray, bonds: np.ndarray):
-    """Per chain: Rg^2, centre of mass (xyz), stored-length fraction."""
+    """Per chain: Rg^2, centre of mass (xyz), stored-length fraction.  For
+    linear chains the end marker is no bond: ComputeSL divides by N - 1
+    (LoadPTL, analysis/mode_io.c:590-597, sets polSize = nMono - 1)."""
     xyz = to_xyz(unwrapped_tuv(start, bonds))
     cms = xyz.mean(axis=1)
     rg2 = ((xyz - cms[:, None, :]) ** 2).sum(axis=2).mean(axis=1)
-    sl = (bonds == 0).mean(axis=1)
+    sl = (bonds[:, :-1] == 0).mean(axis=1) if is_linear(bonds) else (bonds == 0).mean(axis=1)
     return rg2, cms, sl
 
 

@@ -82,6 +82,7 @@ typedef struct orc_replay {
     uint32_t* lat;            /* L^3 site words */
     uint32_t* rec;            /* 4 words per chain: site, count, offset, 0 */
     uint64_t accepted, attempted;
+    int linear;               /* 1: linear chains (last run's b_out is 0xf) */
 } orc_replay;
 
 orc_replay* orc_replay_new(const orc_geom* g, int N, int P, uint32_t seed, uint32_t salt);
@@ -91,6 +92,8 @@ int  orc_replay_load(orc_replay* r, const int32_t* start, const uint8_t* bonds);
 /* Walk chains back out of the site words. 0 = ok, else integrity code. */
 int  orc_replay_export(const orc_replay* r, int32_t* start, uint8_t* bonds);
 void orc_replay_steps(orc_replay* r, long nsteps);
+/* Linear chains (set before load). */
+void orc_replay_set_linear(orc_replay* r, int linear);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,18 @@
  *     Move and reverse move share the anchor, all sites touched lie within
  *     one bond of P, and same-colour anchors are >= 3 bonds apart, so the
  *     substep is conflict-free and each substep kernel is symmetric.
+ *
+ * Linear chains (efpol built with POL_TYPE=POL_LIN): bond N-1 is the end
+ * marker 0xf, stored as b_out of the chain's last run, and monomer 0 is the
+ * first monomer of its run (offset 0).  The move above then covers the last
+ * monomer (rows (u, 0xf) and (0, 0xf) of efpol's table); slot 1 at a last
+ * run has no next run and is null.  Monomer 0 has no predecessor: it moves
+ * about monomer 1 (efpol's rows (0xf, x)).  After its regular attempt, an
+ * anchor holding a chain's monomer 0 draws word 0 of
+ * ctr {t, d, k | 0x20000000, a}: bit 0 set -> one attempt with option bits
+ * 1-4 in row (0xf, run length > 1 ? 0 : b_out): either monomer 0 leaves
+ * its run to the empty site P - u (new bond u), or, alone on P, joins the
+ * front of the next run.  All sites touched lie within one bond of P.
  */
 #include "oracle.h"
 
@@ -102,6 +114,7 @@ static int replay_op(orc_replay* r, const dom* D, int x, int y, int z, uint32_t 
         src1 = 0;
         src2 = bo;
     } else {
+        if (bo == 15) return 0;            /* last run of a linear chain: no next run */
         if (!dnbr(D, x, y, z, bo, &bx, &by, &bz)) return 0;
         iB = dsite(D, bx, by, bz);
         wB = lat[iB];
@@ -160,6 +173,43 @@ static int replay_op(orc_replay* r, const dom* D, int x, int y, int z, uint32_t 
     return 1;
 }
 
+/* Monomer 0 of a linear chain, whose run sits on the anchor (see header). */
+static int replay_head(orc_replay* r, const dom* D, int x, int y, int z, uint32_t r4)
+{
+    uint32_t* lat = r->lat;
+    const size_t iP = dsite(D, x, y, z);
+    const uint32_t wP = lat[iP];
+    const uint32_t chain = wP >> 5, cP = r->rec[4 * (size_t)chain + 1], bo = wP & 15;
+    const uint32_t e = g_tab[(15u << 8) | ((cP >= 2 ? 0u : bo) << 4) | r4];
+    if (!e) return 0;
+    const uint32_t d2 = e >> 4;
+    int nx, ny, nz;
+    if (cP >= 2) {
+        /* monomer 0 leaves to P - d2, its bond to monomer 1 becoming d2 */
+        if (!dnbr(D, x, y, z, (~d2) & 15u, &nx, &ny, &nz)) return 0;
+        const size_t iY = dsite(D, nx, ny, nz);
+        if (lat[iY]) return 0;
+        lat[iP] = bo | ((cP - 1) << CSH);
+        lat[iY] = d2 | LBIT | (chain << 5);
+        r->rec[4 * (size_t)chain + 0] = (uint32_t)iY;
+        r->rec[4 * (size_t)chain + 1] = 1;
+    } else {
+        /* alone on P: monomer 0 joins the front of the next run */
+        if (!dnbr(D, x, y, z, bo, &nx, &ny, &nz)) return 0;
+        const size_t iB = dsite(D, nx, ny, nz);
+        const uint32_t wB = lat[iB];
+        lat[iP] = 0;
+        lat[iB] = (wB & 15) | LBIT | (chain << 5);
+        r->rec[4 * (size_t)chain + 0] = (uint32_t)iB;
+        r->rec[4 * (size_t)chain + 1] = (wB >> CSH) + 1;
+    }
+    r->rec[4 * (size_t)chain + 2] = 0;
+    r->accepted++;
+    return 1;
+}
+
+void orc_replay_set_linear(orc_replay* r, int linear) { r->linear = linear ? 1 : 0; }
+
 orc_replay* orc_replay_new(const orc_geom* g, int N, int P, uint32_t seed, uint32_t salt)
 {
     tab_init();
@@ -196,15 +246,16 @@ int orc_replay_load(orc_replay* r, const int32_t* start, const uint8_t* bonds)
         const uint8_t* b = bonds + (size_t)p * N;
         int t = start[3 * p], u = start[3 * p + 1], v = start[3 * p + 2];
         int nz = 0;
+        if (r->linear && b[N - 1] != 15) { free(pt); return 4; }
         for (int m = 0; m < N; m++) {
             pt[3 * m] = t; pt[3 * m + 1] = u; pt[3 * m + 2] = v;
-            if (b[m] && !orc_is_valid(b[m])) { free(pt); return 4; }
+            if (b[m] && !orc_is_valid(b[m]) && !(r->linear && m == N - 1)) { free(pt); return 4; }
             int dt, du, dv;
             orc_unit_vec(b[m], &dt, &du, &dv);
             t += dt; u += du; v += dv;
             if (b[m]) nz++;
         }
-        if (gsite(L, t, u, v) != gsite(L, pt[0], pt[1], pt[2]) || nz < 2) { free(pt); return 4; }
+        if (!r->linear && (gsite(L, t, u, v) != gsite(L, pt[0], pt[1], pt[2]) || nz < 2)) { free(pt); return 4; }
         /* runs start at monomers whose predecessor's bond is non-zero */
         int first = -1;
         for (int m = 0; m < N; m++) if (b[(m + N - 1) % N]) { first = m; break; }
@@ -249,9 +300,10 @@ int orc_replay_export(const orc_replay* r, int32_t* start, uint8_t* bonds)
         uint32_t here = cnt - off, cur = site;
         for (;;) {
             uint32_t bo = r->lat[cur] & 15;
-            if (!orc_is_valid(bo) || i + here > (long)N) return 4;
+            if (!(orc_is_valid(bo) || (r->linear && bo == 15)) || i + here > (long)N) return 4;
             for (uint32_t k = 0; k + 1 < here; k++) b[i++] = 0;
             b[i++] = (uint8_t)bo;
+            if (bo == 15) break;      /* end of a linear chain */
             int dt, du, dv;
             orc_unit_vec(bo, &dt, &du, &dv);
             int t = (int)(cur % L), u = (int)((cur / L) % L), v = (int)(cur / ((uint32_t)L * L));
@@ -315,6 +367,11 @@ static void replay_step(orc_replay* r)
                     int x = (((ck - 2 * y - 3 * z) % n) + n) % n + n * j;
                     uint32_t rb = (w >> (8 * q)) & 0xff;
                     replay_op(r, &D, x, y, z, rb & 1, (rb >> 1) & 15);
+                    if (r->linear && (r->lat[dsite(&D, x, y, z)] & LBIT)) {
+                        uint32_t hc[4] = {t, (uint32_t)d, (uint32_t)k | 0x20000000u, (uint32_t)a}, hw[4];
+                        orc_philox(hc, key, hw);
+                        if (hw[0] & 1) replay_head(r, &D, x, y, z, (hw[0] >> 1) & 15);
+                    }
                 }
             }
         }

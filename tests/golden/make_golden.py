@@ -26,6 +26,10 @@ It compiles the reference's efpol from its own sources (oracle/Makefile target
   for three of the TUV files above (compact t=0 rings and relaxed melts);
   ``xyz_efpol_L16_N50_s3_t100_p{0,3,97}.txt.gz`` -- its analysis/tuv2xyz.c
   export of three rings;
+* ``efpol_lin_*`` -- the same for linear chains (the reference built with
+  POL_TYPE=POL_LIN as efpol_lin): ``efpol_lin_L32_N100_s1_t{0,100,200}``,
+  ``efpol_lin_L16_N50_s3_t{0..100}`` and ``efpol_lin_stats_L16_N50.json`` /
+  ``efpol_lin_stats_L32_N100.json``;
 * ``efpol_stats_L16_N50.json`` / ``efpol_stats_L32_N100.json`` -- ensemble
   statistics of reference efpol runs (16 and 8 distinct seeds) computed with
   oracle/observables.py: Rg^2, stored-length fraction, run-length histogram and
@@ -123,10 +127,42 @@ def make_export(refdir, tmp):
             g.write(f.read())
 
 
+def make_linear(refdir, tmp):
+    """efpol_lin: initial melt, short trajectories and ensemble statistics."""
+    lin = os.path.join(refdir, "efpol_lin")
+    d = run_efpol(lin, 1, 32, 100, 200, 100, os.path.join(tmp, "lin"))
+    for t in (0, 100, 200):
+        with open(os.path.join(d, f"t={t}_dev=0.res"), "rb") as f, \
+                gzip.GzipFile(os.path.join(HERE, f"efpol_lin_L32_N100_s1_t{t}.res.gz"), "wb", mtime=0) as g:
+            g.write(f.read())
+    d = run_efpol(lin, 3, 16, 50, 100, 10, os.path.join(tmp, "lin"))
+    for t in range(0, 101, 10):
+        with open(os.path.join(d, f"t={t}_dev=0.res"), "rb") as f, \
+                gzip.GzipFile(os.path.join(HERE, f"efpol_lin_L16_N50_s3_t{t}.res.gz"), "wb", mtime=0) as g:
+            g.write(f.read())
+    write_stats(lin, "efpol_lin", "reference efpol_lin (cpupol, POL_LIN, sl_equal), built from source",
+                [(16, 50, 20000, 100, 2000, range(301, 333, 2)), (32, 100, 10000, 100, 3000, range(401, 417, 2))],
+                os.path.join(tmp, "lin_stats"))
+
+
+def write_stats(binary, prefix, engine, cases, tmp):
+    for (L, N, tmax, interval, therm, seeds) in cases:
+        per_seed = []
+        for s in seeds:
+            d = run_efpol(binary, s, L, N, tmax, interval, tmp)
+            rg, sl, hist, msd = stats_of_run(d, tmax, interval, L, therm)
+            per_seed.append({"seed": s, "rg2": rg, "sl_frac": sl, "run_hist": hist, "msd": msd})
+            shutil.rmtree(os.path.dirname(d))
+        out = {"engine": engine, "L": L, "N": N, "density": 1.2, "steps": tmax, "interval": interval, "therm": therm,
+               "msd_lags_intervals": STAT_LAGS, "per_seed": per_seed}
+        with open(os.path.join(HERE, f"{prefix}_stats_L{L}_N{N}.json"), "w") as f:
+            json.dump(out, f, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["all", "ptl", "double", "export"], default="all")
+    ap.add_argument("--only", choices=["all", "ptl", "double", "export", "linear"], default="all")
     args = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={args.ref}"], check=True,
                    stdout=subprocess.DEVNULL)
@@ -142,6 +178,9 @@ def main():
             return
         if args.only == "export":
             make_export(refdir, tmp)
+            return
+        if args.only == "linear":
+            make_linear(refdir, tmp)
             return
         for name, code in MODELS.items():
             raw = os.path.join(tmp, f"tab_{name}.bin")
@@ -164,6 +203,7 @@ def main():
         make_ptl(refdir, efpol, tmp)
         make_double(efpol, tmp)
         make_export(refdir, tmp)
+        make_linear(refdir, tmp)
 
         # efpol's seeding drops bit 0 of every Tausworthe word (util/rng.h:13-20,
         # 26-31), so seeds 2k and 2k+1 give the same run: use odd seeds only.

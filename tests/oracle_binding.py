@@ -40,6 +40,7 @@ def lib():
         L.orc_replay_load.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_replay_export.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_replay_steps.argtypes = [C.c_void_p, C.c_long]
+        L.orc_replay_set_linear.argtypes = [C.c_void_p, C.c_int]
         _LIB = L
     return _LIB
 
@@ -106,10 +107,11 @@ class Geom(C.Structure):
 class Replay:
     """Host replay of the GPU sweep schedule (bit-exact twin of the kernels)."""
 
-    def __init__(self, L, N, P, seed, salt=0, periodic=True, tile=(32, 32, 32), ncol=16):
+    def __init__(self, L, N, P, seed, salt=0, periodic=True, tile=(32, 32, 32), ncol=16, linear=False):
         self.L, self.N, self.P = L, N, P
         g = Geom(L, 1 if periodic else 0, tile[0], tile[1], tile[2], ncol)
         self.h = lib().orc_replay_new(C.byref(g), N, P, seed, salt)
+        lib().orc_replay_set_linear(self.h, 1 if linear else 0)
 
     def load(self, start, bonds):
         start = np.ascontiguousarray(start, dtype=np.int32)
@@ -130,7 +132,7 @@ class Replay:
         class R(C.Structure):
             _fields_ = [("g", Geom), ("N", C.c_int), ("P", C.c_int), ("seed", C.c_uint32), ("salt", C.c_uint32),
                         ("step", C.c_uint64), ("lat", C.POINTER(C.c_uint32)), ("rec", C.POINTER(C.c_uint32)),
-                        ("accepted", C.c_uint64), ("attempted", C.c_uint64)]
+                        ("accepted", C.c_uint64), ("attempted", C.c_uint64), ("linear", C.c_int)]
         return R.from_address(self.h)
 
     def lattice(self):

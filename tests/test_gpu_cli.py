@@ -138,3 +138,40 @@ def test_gpupol_doubling_flow_with_scaleup(tmp_path):
     assert L == 32 and bonds.shape == (98, 400)
     e = Efpol(32, 400, 98, 0)
     assert e.read(obs.format_tuv(L, start, bonds)) == 0 and e.check() == 0
+
+
+def test_efpol_lin_cli(tmp_path):
+    """efpol_lin: the reference's efpol built for linear chains (do_run.sh
+    runs efpol_$POL_TYPE with POL_TYPE=lin): t=0 file byte-identical, valid
+    linear chains after, 'Polytype = lin', and doubling refused (193)."""
+    out = tmp_path / "run"
+    r = subprocess.run([os.path.join(BIN, "efpol_lin"), "1", str(out), "1.2", "200", "100", "100", "0", "32",
+                        "sl_equal"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    d = out / "N_100"
+    ref0 = gzip.open(os.path.join(GOLD, "efpol_lin_L32_N100_s1_t0.res.gz"), "rt").read()
+    assert (d / "t=0_dev=0.res").read_text() == ref0
+    for t in (100, 200):
+        L, start, bonds = obs.parse_tuv((d / f"t={t}_dev=0.res").read_text())
+        assert (bonds[:, -1] == 15).all()
+        e = Efpol(32, 100, start.shape[0], 0, pol_type=2)
+        assert e.read(obs.format_tuv(L, start, bonds)) == 0 and e.check() == 0
+    s = (d / "simulation_settings.txt").read_text()
+    assert "Polytype = lin\n" in s and [ln.split(" = ")[0] for ln in s.splitlines()] == EFPOL_KEYS
+    r = subprocess.run([os.path.join(BIN, "efpol_lin"), "1", str(tmp_path / "x"), "1.2", "10", "5", "800", "1", "32",
+                        "sl_equal"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 193
+
+
+def test_gpupol_lin_cli_resume(tmp_path):
+    exe = os.path.join(BIN, "gpupol3_cuda_lin")
+    a, b = tmp_path / "a", tmp_path / "b"
+    args = ["60", "{T}", "4", "{D}", "1.2", "0", "50", "16", "16", "16"]
+    run = lambda T, D: subprocess.run([exe] + [x.format(T=T, D=D) for x in args], capture_output=True, text=True,
+                                      timeout=120)
+    assert run(200, a).returncode == 0
+    assert run(100, b).returncode == 0
+    assert run(100, b).returncode == 0
+    for t in (0, 50, 100, 150, 200):
+        assert (a / f"t={t}_dev=0.res").read_text() == (b / f"t={t}_dev=0.res").read_text(), t
+    assert "Polytype = lin" in (a / "simulation_settings.txt").read_text()

@@ -1,7 +1,8 @@
 """Ensemble statistics of the GPU engine against the reference's CPU efpol.
 
-tests/golden/efpol_stats_*.json hold per-seed statistics of reference efpol
-runs (built from the reference sources, tests/golden/make_golden.py).  The
+tests/golden/efpol_stats_*.json and efpol_lin_stats_*.json hold per-seed
+statistics of reference efpol_ring and efpol_lin runs (built from the
+reference sources, tests/golden/make_golden.py).  The
 GPU runs the same melts (same L, N, density, initial state, step count and
 dump interval) with other seeds -- its parallel schedule cannot reproduce
 efpol's random stream -- and the ensemble means must agree within the
@@ -28,8 +29,8 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 Z = 4.0
 
 
-def gpu_ensemble(L, N, steps, interval, therm, lags, seeds):
-    b = elp.Batch([dict(L=L, N=N, seed=s, steps_per_launch=interval) for s in seeds])
+def gpu_ensemble(L, N, steps, interval, therm, lags, seeds, linear=0):
+    b = elp.Batch([dict(L=L, N=N, seed=s, steps_per_launch=interval, linear=linear) for s in seeds])
     b.init_melts()
     nseed = len(seeds)
     cms = [[] for _ in range(nseed)]
@@ -65,12 +66,14 @@ def compare(ref, gpu, key, idx=None):
     return abs(a.mean() - g.mean()), se, a.mean(), g.mean()
 
 
-@pytest.mark.parametrize("name,seeds", [("efpol_stats_L16_N50.json", range(2001, 2009)),
-                                        ("efpol_stats_L32_N100.json", range(3001, 3005))])
-def test_statistics_match_reference_efpol(name, seeds):
+@pytest.mark.parametrize("name,seeds,linear", [("efpol_stats_L16_N50.json", range(2001, 2009), 0),
+                                               ("efpol_stats_L32_N100.json", range(3001, 3005), 0),
+                                               ("efpol_lin_stats_L16_N50.json", range(4001, 4009), 1),
+                                               ("efpol_lin_stats_L32_N100.json", range(5001, 5005), 1)])
+def test_statistics_match_reference_efpol(name, seeds, linear):
     ref = json.load(open(os.path.join(GOLD, name)))
     gpu = gpu_ensemble(ref["L"], ref["N"], ref["steps"], ref["interval"], ref["therm"], ref["msd_lags_intervals"],
-                       list(seeds))
+                       list(seeds), linear)
     rows = []
     checks = [("rg2", None), ("sl_frac", None)] + [("run_hist", i) for i in range(4)] + \
              [("msd", i) for i in range(len(ref["msd_lags_intervals"]))]

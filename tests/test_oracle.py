@@ -48,21 +48,24 @@ def test_table_is_symmetric_for_rings():
         assert mult.get((d[0], d[1], (s1, s2)), 0) == m
 
 
-def test_initial_state_byte_identical():
-    ref = gold_text("efpol_L32_N100_s1_t0.res.gz")
-    e = Efpol(32, 100, 393, 1)
+@pytest.mark.parametrize("name,pol_type", [("efpol_L32_N100_s1_t0.res.gz", 1), ("efpol_lin_L32_N100_s1_t0.res.gz", 2)])
+def test_initial_state_byte_identical(name, pol_type):
+    ref = gold_text(name)
+    e = Efpol(32, 100, 393, 1, pol_type=pol_type)
     e.create()
     assert e.check() == 0
     assert e.tuv() == ref
 
 
-@pytest.mark.parametrize("L,N,seed,times,fmt", [
-    (16, 50, 3, list(range(0, 101, 10)), "efpol_L16_N50_s3_t{}.res.gz"),
-    (32, 100, 1, [0, 100, 200], "efpol_L32_N100_s1_t{}.res.gz"),
+@pytest.mark.parametrize("L,N,seed,times,fmt,pol_type", [
+    (16, 50, 3, list(range(0, 101, 10)), "efpol_L16_N50_s3_t{}.res.gz", 1),
+    (32, 100, 1, [0, 100, 200], "efpol_L32_N100_s1_t{}.res.gz", 1),
+    (16, 50, 3, list(range(0, 101, 10)), "efpol_lin_L16_N50_s3_t{}.res.gz", 2),
+    (32, 100, 1, [0, 100, 200], "efpol_lin_L32_N100_s1_t{}.res.gz", 2),
 ])
-def test_trajectory_bit_exact(L, N, seed, times, fmt):
+def test_trajectory_bit_exact(L, N, seed, times, fmt, pol_type):
     P = max(1, int(1.2 * L ** 3 / N + 0.5))
-    e = Efpol(L, N, P, seed)
+    e = Efpol(L, N, P, seed, pol_type=pol_type)
     e.create()
     prev = 0
     for t in times:
