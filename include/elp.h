@@ -87,7 +87,10 @@ elp_status elp_init_melt(elp_ctx* ctx);
 
 /* Load rings from chain form: start[3*P] = (t,u,v) of monomer 0 in [0,L),
  * bonds[P*N] = 4-bit bond codes (TUV order).  `step` sets the absolute step
- * counter, so a run resumed from a dump continues the same random stream. */
+ * counter, so a run resumed from a dump continues the same random stream.
+ * Only the chains are copied to the device, where the site words are built.
+ * Invalid chains return ELP_ERR_INTEGRITY and leave the context with no
+ * configuration loaded. */
 elp_status elp_load_chains(elp_ctx* ctx, const int32_t* start, const uint8_t* bonds, uint64_t step);
 
 /* Load a TUV file (LT/LU/LV/np/maxPolLength header, len= blocks). */

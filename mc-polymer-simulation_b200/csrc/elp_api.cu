@@ -146,22 +146,29 @@ static elp_status upload(elp_ctx* c, const uint32_t* lat, const uint32_t* rec, u
 extern "C" elp_status elp_load_chains(elp_ctx* c, const int32_t* start, const uint8_t* bonds, uint64_t step)
 {
     if (!c || !start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
-    size_t S = (size_t)c->g.L * c->g.L * c->g.L;
-    std::vector<uint32_t> lat(S), rec((size_t)c->P * ELP_REC_WORDS);
-    int rc = elp_chains_to_sites(c->g.L, c->N, c->P, start, bonds, lat.data(), rec.data(), c->linear);
-    if (rc == 3) return elp_fail(ELP_ERR_INTEGRITY, "two rings or two runs of a ring share a site (code 3)");
-    if (rc) return elp_fail(ELP_ERR_INTEGRITY, "invalid ring: bad bond, not closed, or on a single site (code 4)");
-    return upload(c, lat.data(), rec.data(), step);
+    ELP_CUDA_TRY(cudaSetDevice(c->device));
+    // the lattice is rebuilt in place on the device: until that succeeds the
+    // context holds no configuration
+    c->loaded = 0;
+    elp_status st = elp_build_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, start, bonds, &c->wb, c->stream);
+    if (st) return st;
+    ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, step));
+    ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->loaded = 1;
+    return ELP_OK;
 }
 
 extern "C" elp_status elp_init_melt(elp_ctx* c)
 {
     if (!c) return elp_fail(ELP_ERR_ARG, "null context");
-    std::vector<int32_t> start((size_t)c->P * 3);
-    std::vector<uint8_t> bonds((size_t)c->P * c->N);
-    if (elp_initial_chains(c->g.L, c->N, c->P, start.data(), bonds.data(), c->linear))
-        return elp_fail(ELP_ERR_ARG, "initial grid cannot hold %d rings of %d in L=%d", c->P, c->N, c->g.L);
-    return elp_load_chains(c, start.data(), bonds.data(), 0);
+    ELP_CUDA_TRY(cudaSetDevice(c->device));
+    c->loaded = 0;
+    elp_status st = elp_init_melt_device(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, c->stream);
+    if (st) return st;
+    ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, 0));
+    ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->loaded = 1;
+    return ELP_OK;
 }
 
 extern "C" elp_status elp_set_state(elp_ctx* c, const uint32_t* words, const uint32_t* records, uint64_t step)

@@ -87,7 +87,7 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
     if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || b->nsm < 1) b->nsm = 148;
 
     // resolve every melt; group by geometry, steps per launch and kernel choice
-    std::map<std::tuple<int, int, int, int, int, int, int, int>, int> key2g;
+    std::map<std::tuple<int, int, int, int, int, int, int, int, int>, int> key2g;
     std::vector<std::tuple<elp_geometry, int, int>> gdesc;  // geometry, spl, generic
     size_t lat_words = 0, rec_words = 0;
     elp_status st = ELP_OK;
@@ -105,7 +105,8 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
         mm.salt = specs[j].salt;
         const int spl = mm.g.periodic ? (specs[j].steps_per_launch > 0 ? specs[j].steps_per_launch : 1) : 1;
         const int gen = specs[j].kernel == 1;
-        auto key = std::make_tuple(mm.g.periodic, mm.g.L, mm.g.tx, mm.g.ty, mm.g.tz, mm.g.ncol, spl, gen);
+        // rings and linear chains run in different groups (different kernels)
+        auto key = std::make_tuple(mm.g.periodic, mm.g.L, mm.g.tx, mm.g.ty, mm.g.tz, mm.g.ncol, spl, gen, mm.linear);
         auto it = key2g.find(key);
         if (it == key2g.end()) {
             it = key2g.emplace(key, (int)gdesc.size()).first;
@@ -208,15 +209,12 @@ extern "C" elp_status elp_batch_load_chains(elp_batch* b, int32_t j, const int32
     if (st) return st;
     if (!start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
     Member& mm = b->m[(size_t)j];
-    const size_t S = (size_t)mm.g.L * mm.g.L * mm.g.L;
-    std::vector<uint32_t> lat(S), rec((size_t)mm.P * ELP_REC_WORDS);
-    int rc = elp_chains_to_sites(mm.g.L, mm.N, mm.P, start, bonds, lat.data(), rec.data(), mm.linear);
-    if (rc == 3) return elp_fail(ELP_ERR_INTEGRITY, "melt %d: two runs share a site (code 3)", j);
-    if (rc) return elp_fail(ELP_ERR_INTEGRITY, "melt %d: invalid ring (code 4)", j);
     ELP_CUDA_TRY(cudaSetDevice(b->device));
     cudaStream_t s = b->streams[(size_t)mm.group];
-    ELP_CUDA_TRY(cudaMemcpyAsync(mm.lat, lat.data(), S * 4, cudaMemcpyHostToDevice, s));
-    ELP_CUDA_TRY(cudaMemcpyAsync(mm.rec, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice, s));
+    // built in place on the device; until that succeeds the melt holds no configuration
+    mm.loaded = 0;
+    st = elp_build_melt(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, mm.linear, start, bonds, &b->wb, s);
+    if (st) return elp_fail(st, "melt %d: %s", j, elp_last_error());
     ELP_CUDA_TRY(elp_group_set_step(b->groups[(size_t)mm.group], mm.index, step));
     ELP_CUDA_TRY(cudaStreamSynchronize(s));
     mm.loaded = 1;
@@ -226,16 +224,17 @@ extern "C" elp_status elp_batch_load_chains(elp_batch* b, int32_t j, const int32
 extern "C" elp_status elp_batch_init_melts(elp_batch* b)
 {
     if (!b) return elp_fail(ELP_ERR_ARG, "null batch");
+    ELP_CUDA_TRY(cudaSetDevice(b->device));
     for (size_t j = 0; j < b->m.size(); j++) {
-        const Member& mm = b->m[j];
-        std::vector<int32_t> start((size_t)mm.P * 3);
-        std::vector<uint8_t> bonds((size_t)mm.P * mm.N);
-        if (elp_initial_chains(mm.g.L, mm.N, mm.P, start.data(), bonds.data(), mm.linear))
-            return elp_fail(ELP_ERR_ARG, "melt %zu: initial grid cannot hold %d rings of %d in L=%d", j, mm.P, mm.N,
-                            mm.g.L);
-        elp_status st = elp_batch_load_chains(b, (int32_t)j, start.data(), bonds.data(), 0);
-        if (st) return st;
+        Member& mm = b->m[j];
+        cudaStream_t s = b->streams[(size_t)mm.group];
+        mm.loaded = 0;
+        elp_status st = elp_init_melt_device(mm.lat, mm.rec, mm.g.L, mm.N, mm.P, mm.linear, s);
+        if (st) return elp_fail(st, "melt %zu: %s", j, elp_last_error());
+        ELP_CUDA_TRY(elp_group_set_step(b->groups[(size_t)mm.group], mm.index, 0));
     }
+    for (cudaStream_t s : b->streams) ELP_CUDA_TRY(cudaStreamSynchronize(s));
+    for (Member& mm : b->m) mm.loaded = 1;
     return ELP_OK;
 }
 

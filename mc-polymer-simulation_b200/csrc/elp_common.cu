@@ -125,7 +125,7 @@ void elp_walk_bufs_free(elp_walk_bufs* b)
     *b = elp_walk_bufs();
 }
 
-static elp_status ensure(elp_walk_bufs* b, int P, int N, size_t sites)
+elp_status elp_walk_bufs_reserve(elp_walk_bufs* b, int P, int N, size_t sites)
 {
     if ((size_t)P > b->cap_rings) {
         cudaFree(b->d_start); cudaFree(b->d_status);
@@ -156,7 +156,7 @@ static elp_status ensure(elp_walk_bufs* b, int P, int N, size_t sites)
 elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                            int32_t* start, uint8_t* bonds, cudaStream_t s)
 {
-    elp_status st = ensure(b, P, N, 0);
+    elp_status st = elp_walk_bufs_reserve(b, P, N, 0);
     if (st) return st;
     WalkArgs w;
     memset(&w, 0, sizeof(w));
@@ -178,7 +178,7 @@ elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N
                           int32_t* code, cudaStream_t s)
 {
     size_t S = (size_t)L * L * L;
-    elp_status st = ensure(b, P, N, S);
+    elp_status st = elp_walk_bufs_reserve(b, P, N, S);
     if (st) return st;
     ELP_CUDA_TRY(cudaMemsetAsync(b->d_visit, 0, S * sizeof(uint32_t), s));
     ELP_CUDA_TRY(cudaMemsetAsync(b->d_cnt, 0, 8 * sizeof(unsigned long long), s));

@@ -38,6 +38,16 @@ struct elp_walk_bufs {
     size_t bytes = 0;
 };
 void elp_walk_bufs_free(elp_walk_bufs* b);
+// Grow the scratch to P chains of N and `sites` visit counters.
+elp_status elp_walk_bufs_reserve(elp_walk_bufs* b, int P, int N, size_t sites);
+// Build a melt's site words and chain records on the device from host chains
+// (start[3*P], bonds[P*N]); ELP_ERR_INTEGRITY (codes 3/4) for invalid chains,
+// which leave the lattice partly written.
+elp_status elp_build_melt(uint32_t* lat, uint32_t* rec, int L, int N, int P, int linear, const int32_t* start,
+                          const uint8_t* bonds, elp_walk_bufs* wb, cudaStream_t s);
+// The reference initial melt (CreatePolymers) written on the device,
+// stream-ordered: no transfer, no host wait.
+elp_status elp_init_melt_device(uint32_t* lat, uint32_t* rec, int L, int N, int P, int linear, cudaStream_t s);
 
 // Rebuild rings (start[3P], bonds[P*N]) of one melt into host buffers.
 elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,

@@ -24,6 +24,7 @@ Sweep2Launch make_launch(const elp_group* G, int nsteps, uint32_t step_base, int
     for (const BatchJob& j : G->jobs) {
         double m = j.nchains * sites / box;
         if (m > l.max_runs_per_domain) l.max_runs_per_domain = m;
+        if (j.linear) l.linear = 1;
     }
     l.args.jobs = G->d_jobs;
     l.args.items = G->d_items;

@@ -199,10 +199,11 @@ int elp_get_npol(double density, int N, long sites)
     return (int)(density * (double)sites / (double)N + 0.5);
 }
 
-// CreatePolymers, cpupol/efpol_init.c:239-283: rings on a delta-spaced grid,
-// monomer 0 alone, bond +v, the other N-1 monomers stored on the next site,
-// closing bond -v.  Returns 0, or 1 if the grid cannot hold P rings.
-int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds, int linear)
+// CreatePolymers, cpupol/efpol_init.c:239-283: chains on a delta-spaced
+// grid (monomer 0 alone, bond +v, the other N-1 monomers stored on the next
+// site; the site words are written by init_kernel, elp_build.cu).  The
+// grid's spacing and extents; returns 0, or 1 if it cannot hold P chains.
+int elp_initial_grid(int L, int N, int P, int* delta_out, int* nt_out, int* nv_out)
 {
     if (N < 3 || P < 1) return 1;
     int delta;
@@ -213,69 +214,9 @@ int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds, int 
     if (delta < 1 || delta >= L) return 1;
     int nt = L / delta, nv = L / (delta + 1);
     if ((long)nt * nv * (L / delta) < P) return 1;
-    for (int p = 0; p < P; p++) {
-        start[3 * p] = delta * (p % nt);
-        start[3 * p + 1] = delta * (p / nt / nv);
-        start[3 * p + 2] = (delta + 1) * ((p / nt) % nv);
-        uint8_t* b = bonds + (size_t)p * N;
-        memset(b, 0, (size_t)N);
-        b[0] = 0x4;
-        b[N - 1] = linear ? 0xf : 0xb;   // end marker, or the -v bond closing the ring
-    }
+    *delta_out = delta;
+    *nt_out = nt;
+    *nv_out = nv;
     return 0;
 }
 
-static inline uint32_t wrap_site(int L, long t, long u, long v)
-{
-    t %= L; u %= L; v %= L;
-    if (t < 0) t += L;
-    if (u < 0) u += L;
-    if (v < 0) v += L;
-    return (uint32_t)(t + (long)L * (u + (long)L * v));
-}
-
-int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t* bonds, uint32_t* lat, uint32_t* rec,
-                        int linear)
-{
-    size_t S = (size_t)L * L * L;
-    memset(lat, 0, S * sizeof(uint32_t));
-    std::vector<uint32_t> pos((size_t)N);
-    for (int p = 0; p < P; p++) {
-        const uint8_t* b = bonds + (size_t)p * N;
-        long t = start[3 * p], u = start[3 * p + 1], v = start[3 * p + 2];
-        if (t < 0 || u < 0 || v < 0 || t >= L || u >= L || v >= L) return 4;
-        int nz = 0;
-        if (linear && b[N - 1] != 0xf) return 4;
-        for (int m = 0; m < N; m++) {
-            pos[(size_t)m] = wrap_site(L, t, u, v);
-            if (b[m] && !elp_valid_bond(b[m]) && !(linear && m == N - 1)) return 4;
-            t += elp_bt(b[m]); u += elp_bu(b[m]); v += elp_bv(b[m]);
-            nz += b[m] ? 1 : 0;
-        }
-        // a ring closes on itself; a linear chain's runs end with the marker's run
-        if (!linear && (wrap_site(L, t, u, v) != pos[0] || nz < 2)) return 4;
-        int first = 0;
-        while (!b[(first + N - 1) % N]) first++;
-        int m = first, done = 0;
-        while (done < N) {
-            int len = 1;
-            while (b[(m + len - 1) % N] == 0) len++;
-            uint32_t site = pos[(size_t)m];
-            if (lat[site]) return 3;
-            uint32_t bo = b[(m + len - 1) % N];
-            int off0 = (N - m) % N;
-            if (off0 < len) {
-                lat[site] = bo | ELP_LBIT | ((uint32_t)p << 5);
-                rec[ELP_REC_WORDS * p + 0] = site;
-                rec[ELP_REC_WORDS * p + 1] = (uint32_t)len;
-                rec[ELP_REC_WORDS * p + 2] = (uint32_t)off0;
-                rec[ELP_REC_WORDS * p + 3] = 0;
-            } else {
-                lat[site] = bo | ((uint32_t)len << ELP_CSHIFT);
-            }
-            done += len;
-            m = (m + len) % N;
-        }
-    }
-    return 0;
-}

@@ -69,8 +69,8 @@ void elp_layout(const elp_geometry* g, elp_smem_layout* lay);
 void elp_philox_host(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void elp_build_table(uint8_t tab[4096]);
 int elp_get_npol(double density, int N, long sites);
-// CreatePolymers-equivalent start layout (cpupol/efpol_init.c:239-283).
-int elp_initial_chains(int L, int N, int P, int32_t* start, uint8_t* bonds, int linear);
-// chains -> site words + records; returns 0, 3 (two runs on one site), 4 (bad chain)
-int elp_chains_to_sites(int L, int N, int P, const int32_t* start, const uint8_t* bonds, uint32_t* lat,
-                        uint32_t* rec, int linear);
+// The grid of CreatePolymers (cpupol/efpol_init.c:239-283): chain p starts at
+// (delta (p % nt), delta (p / nt / nv), (delta + 1) ((p / nt) % nv)).
+// Returns 0, or 1 if it cannot hold P chains.
+int elp_initial_grid(int L, int N, int P, int* delta, int* nt, int* nv);
+

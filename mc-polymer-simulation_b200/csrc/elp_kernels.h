@@ -62,6 +62,7 @@ struct Sweep2Launch {
     BatchLaunch args;
     int threads_out;               // check_only: block size of the kernel that fits
     size_t smem_out;               // check_only: its dynamic shared memory
+    int linear;                    // 1: some job holds linear chains (kernel with monomer-0 moves)
 };
 
 extern "C" {

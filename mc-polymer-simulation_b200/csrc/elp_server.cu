@@ -236,19 +236,14 @@ static bool admit(elp_server* s)
             fail_job(s, j, ELP_ERR_NOMEM, "device allocation failed");
             continue;
         }
-        std::vector<int32_t> start((size_t)j->P * 3);
-        std::vector<uint8_t> bonds((size_t)j->P * j->spec.N);
-        std::vector<uint32_t> lat(S), rec((size_t)j->P * ELP_REC_WORDS);
-        if (elp_initial_chains(j->g.L, j->spec.N, j->P, start.data(), bonds.data(), 0) ||
-            elp_chains_to_sites(j->g.L, j->spec.N, j->P, start.data(), bonds.data(), lat.data(), rec.data(), 0)) {
+        // the initial melt is written on the device, ordered on the group's
+        // stream behind its running steps: the scheduler does not wait
+        if (elp_init_melt_device(j->lat, j->rec, j->g.L, j->spec.N, j->P, 0, gp->s) != ELP_OK) {
             cudaFreeAsync(j->lat, gp->s);
             cudaFreeAsync(j->rec, gp->s);
             fail_job(s, j, ELP_ERR_ARG, "initial melt does not fit the box");
             continue;
         }
-        cudaMemcpyAsync(j->lat, lat.data(), S * 4, cudaMemcpyHostToDevice, gp->s);
-        cudaMemcpyAsync(j->rec, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice, gp->s);
-        if (cudaStreamSynchronize(gp->s) != cudaSuccess) return false;
         for (size_t g = 0; g < s->groups.size(); g++)
             if (s->groups[g].get() == gp) j->group = (int)g;
         gp->members.push_back(j);

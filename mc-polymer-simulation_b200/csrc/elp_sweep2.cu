@@ -68,7 +68,7 @@ extern __shared__ __align__(16) uint32_t g_smem[];
 // Anchor q takes its random byte at bit offset bsh[q] of the Philox word w.
 // Shared-memory word indices: lattice at 0, transition table (bytes) at
 // TABW words, neighbour offsets at OFFW words.
-template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW>
+template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW, bool LIN>
 __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, const int (&base)[K], const int (&rot)[K],
                                         const int (&clsyz)[K], const int (&xj)[K], const int (&bsh)[K],
                                         const int (&an)[K], int c, uint32_t w, int L, bool lin, uint32_t t, int d,
@@ -166,7 +166,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         if (ok && s) S[pB[q]] = nB;
         if (ok && d1) S[pY[q]] = nY;
         if (ok) S[p[q]] = nP;
-        wP[q] = ok ? nP : wP[q];
+        if (LIN) wP[q] = ok ? nP : wP[q];
         acc += ok ? 1 : 0;
     }
     // linear chains: monomer 0 has no predecessor and moves about monomer 1,
@@ -174,7 +174,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
     // with probability 1/2 (bit 0 of its own Philox word) one option of row
     // (0xf, run length > 1 ? 0 : b_out) -- it leaves to the empty site P - u
     // (its bond to monomer 1 becoming u), or, alone on P, joins the next run
-    if (lin) {
+    if (LIN && lin) {
         const uint8_t* htab = reinterpret_cast<const uint8_t*>(g_smem + HTABW);
 #pragma unroll
         for (int q = 0; q < K; q++) {
@@ -214,7 +214,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
 // more warps (latency hiding when a domain has few anchors per SM).  The
 // random stream does not depend on K: anchor a = g + q * G always takes byte
 // q of Philox word (k & 3) of counter {t, d, k / 4, g}.
-template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB>
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB, bool LIN>
 __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 {
     using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K>;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         uint32_t* rec = J.rec;
         const int nchains = J.nchains;
         const uint2 key = make_uint2(J.seed, J.salt);
-        const bool lin = J.linear != 0;
+        const bool lin = LIN && J.linear != 0;   // the ring instantiation has no monomer-0 moves
         const int ntx = J.ntx, nty = J.nty;
         Dom D;
         D.S = S; D.tab = tab; D.rec = rec;
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++) {
                     if (active)
-                        accepted += substepK<K, PER, NC, TABW, OFFW, HTABW>(
+                        accepted += substepK<K, PER, NC, TABW, OFFW, HTABW, LIN>(
                             slot_off, slot_site, base, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d,
                             k + kk, key);
                     __syncthreads();
@@ -432,11 +432,11 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 }  // namespace elp
 
 // ---- dispatch ----------------------------------------------------------------
-template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB>
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB, bool LIN>
 static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 {
     using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K>;
-    auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, THREADS, MINB>;
+    auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, THREADS, MINB, LIN>;
     if (l->check_only) {
         // expected monomer-0 runs per domain must stay far inside the slot table
         const double m = l->max_runs_per_domain;
@@ -468,7 +468,8 @@ extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
 #define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_)                                        \
     if (g.tx == X_ && g.ty == Y_ && g.tz == Z_ && g.periodic == PER_ && g.ncol == NC_ && l->sx == SX_ &&       \
         l->sxy == SXY_)                                                                                        \
-        return launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_>(l, s);
+        return l->linear ? launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, true>(l, s)        \
+                         : launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, false>(l, s);
     SHAPE(32, 32, 32, 0, 16, 35, 1190, 2048, 2, 1024, 1)
     SHAPE(32, 32, 16, 0, 16, 35, 1190, 1024, 1, 1024, 1)
     SHAPE(16, 16, 16, 0, 16, 19, 342, 512, 1, 256, 4)

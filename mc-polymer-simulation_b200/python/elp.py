@@ -258,9 +258,13 @@ class Melt:
         """cudaStream_t of this melt (e.g. for torch.cuda.ExternalStream)."""
         return lib().elp_stream(self.h) or 0
 
-    def fetch(self):
-        start = np.zeros((self.P, 3), dtype=np.int32)
-        bonds = np.zeros((self.P, self.N), dtype=np.uint8)
+    def fetch(self, start=None, bonds=None):
+        """Rings as (start (P,3) int32, bonds (P,N) uint8), written into the given
+        C-contiguous arrays (e.g. pinned host memory) or into new ones."""
+        start = np.zeros((self.P, 3), dtype=np.int32) if start is None else start
+        bonds = np.zeros((self.P, self.N), dtype=np.uint8) if bonds is None else bonds
+        assert start.shape == (self.P, 3) and start.dtype == np.int32 and start.flags.c_contiguous
+        assert bonds.shape == (self.P, self.N) and bonds.dtype == np.uint8 and bonds.flags.c_contiguous
         check(lib().elp_fetch_chains(self.h, start.ctypes.data, bonds.ctypes.data))
         return start, bonds
 

@@ -201,3 +201,32 @@ def test_specialised_kernels_equal_generic(L, N, kw):
         wb, rb = b.state()
         assert np.array_equal(wa, wb) and np.array_equal(ra, rb)
     assert a.accepted() == b.accepted()
+
+
+@pytest.mark.parametrize("name,L,N,linear", [("efpol_L32_N100_s1_t200", 32, 100, 0),
+                                             ("efpol_L16_N50_s3_t100", 16, 50, 0),
+                                             ("efpol_lin_L32_N100_s1_t200", 32, 100, 1)])
+def test_device_load_builds_the_replay_state(name, L, N, linear):
+    """elp_load_chains builds site words and records on the device from the
+    chains alone; they equal the host replay's load of the same chains."""
+    _, start, bonds = obs.read_tuv(os.path.join(GOLD, name + ".res.gz"))
+    m = elp.Melt(L=L, N=N, seed=1, linear=linear)
+    m.load_chains(start, bonds, 7)
+    r = Replay(L, N, m.P, 1, linear=bool(linear))
+    assert r.load(start, bonds) == 0
+    w, rec = m.state()
+    assert np.array_equal(w, r.lattice()) and np.array_equal(rec, r.records())
+    assert np.any(rec[:, 2] > 0) or linear          # rings with monomer 0 inside a run
+    assert m.step == 7 and m.check() == 0
+
+
+def test_device_load_of_rings_wrapping_the_box():
+    m = elp.Melt(L=16, N=2000, seed=3)
+    m.init_melt()
+    m.run(400)
+    s, b = m.fetch()
+    m2 = elp.Melt(L=16, N=2000, seed=3)
+    m2.load_chains(s, b, 400)
+    w1, r1 = m.state()
+    w2, r2 = m2.state()
+    assert np.array_equal(w1, w2) and np.array_equal(r1, r2)
