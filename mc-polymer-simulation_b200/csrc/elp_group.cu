@@ -120,12 +120,24 @@ cudaError_t elp_group_commit(elp_group* G)
     const int nd = domains_of(G->g);
     const size_t nj = G->jobs.size();
     cudaError_t e;
-    if (G->d_jobs) cudaFree(G->d_jobs);
-    if (G->d_items) cudaFree(G->d_items);
-    G->d_jobs = nullptr;
-    G->d_items = nullptr;
-    if ((e = cudaMalloc((void**)&G->d_jobs, nj * sizeof(BatchJob))) != cudaSuccess) return e;
-    if ((e = cudaMalloc((void**)&G->d_items, nj * nd * sizeof(uint2))) != cudaSuccess) return e;
+    // the tables grow only, stream-ordered: a membership change (the serving
+    // loop commits every few ticks) synchronises nothing but this group
+    if (nj > G->cap_jobs) {
+        if (G->d_jobs && (e = cudaFreeAsync(G->d_jobs, G->stream)) != cudaSuccess) return e;
+        G->d_jobs = nullptr;
+        G->cap_jobs = 0;
+        const size_t cap = nj < 16 ? 16 : 2 * nj;
+        if ((e = cudaMallocAsync((void**)&G->d_jobs, cap * sizeof(BatchJob), G->stream)) != cudaSuccess) return e;
+        G->cap_jobs = cap;
+    }
+    if (nj * nd > G->cap_items) {
+        if (G->d_items && (e = cudaFreeAsync(G->d_items, G->stream)) != cudaSuccess) return e;
+        G->d_items = nullptr;
+        G->cap_items = 0;
+        const size_t cap = nj * nd < 64 ? 64 : 2 * nj * nd;
+        if ((e = cudaMallocAsync((void**)&G->d_items, cap * sizeof(uint2), G->stream)) != cudaSuccess) return e;
+        G->cap_items = cap;
+    }
     std::vector<uint2> items(nj * nd);
     // domain-major order: the first wave of a persistent grid spreads over melts
     for (int d = 0; d < nd; d++)
@@ -212,6 +224,7 @@ cudaError_t elp_group_run(elp_group* G, int64_t nsteps)
 void elp_group_free(elp_group* G)
 {
     if (G->graph) cudaGraphExecDestroy(G->graph);
+    if (G->stream) cudaStreamSynchronize(G->stream);
     cudaFree(G->d_jobs);
     cudaFree(G->d_items);
     cudaFree(G->d_ctr);

@@ -33,6 +33,7 @@ struct elp_group {
     BatchJob* d_jobs = nullptr;
     uint2* d_items = nullptr;
     int nitems = 0;
+    size_t cap_jobs = 0, cap_items = 0;   // grow-only device capacity of the two tables
     uint32_t* d_ctr = nullptr;        // device step counter
     uint64_t steps_done = 0;          // steps since the job table's step0 values
     uint32_t ctr_mirror = 0;          // host copy of *d_ctr

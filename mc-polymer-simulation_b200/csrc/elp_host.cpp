@@ -5,6 +5,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "elp_internal.h"
@@ -83,7 +86,7 @@ static int bank_cost(const elp_geometry* g, int ox, int sx, int sxy)
     return worst;
 }
 
-void elp_layout(const elp_geometry* g, elp_smem_layout* lay)
+static void layout_search(const elp_geometry* g, elp_smem_layout* lay)
 {
     int halo = g->periodic ? 0 : 2;
     int best_sx = 0, best_sxy = 0, best = 1 << 30;
@@ -103,6 +106,27 @@ void elp_layout(const elp_geometry* g, elp_smem_layout* lay)
     lay->anchors = g->ty * g->tz * (g->tx / g->ncol);
     lay->groups = lay->anchors / 4;
     lay->bytes = (size_t)lay->words * 4 + 4096 + 27 * 16 * 4 + 64 * 4;
+}
+
+// The padding search scores hundreds of candidate strides (milliseconds); a
+// geometry's layout is computed once per process and reused (every job
+// submitted to the serving loop resolves its geometry through here).
+void elp_layout(const elp_geometry* g, elp_smem_layout* lay)
+{
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int, int, int>, elp_smem_layout> memo;
+    const auto key = std::make_tuple(g->L, g->periodic, g->tx, g->ty, g->tz, g->ncol);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = memo.find(key);
+        if (it != memo.end()) {
+            *lay = it->second;
+            return;
+        }
+    }
+    layout_search(g, lay);
+    std::lock_guard<std::mutex> lk(mu);
+    memo.emplace(key, *lay);
 }
 
 // ---- Philox4x32-10 (host copy; Salmon et al. SC'11) --------------------------

@@ -1,16 +1,18 @@
 // elp_server.cu -- the serving loop: continuous batching of melt jobs.
 //
-// Jobs (a melt spec, a step count, a dump interval) arrive at any time.  A
-// scheduler thread runs ticks of `quantum` steps.  Between ticks it admits
-// queued jobs whose device memory fits the HBM budget, places them in the
-// group of their domain geometry (elp_group.h) and retires finished ones, so
-// requests that arrive while others are on the GPU join the running mix as
-// memory frees up.  Lattices stay resident between dumps.  At a dump the
-// job's state is copied device-to-device at the end of the tick; rebuilding
-// the rings and the device-to-host copy into pinned memory then run on a side
-// stream while the next tick computes, and host I/O threads format the TUV
-// text.  A job follows the same trajectory alone, in any mix, or through the
-// single-melt API: its kernel, counters and geometry depend only on its spec.
+// Jobs (a melt spec, a step count, a dump interval) arrive at any time.  Each
+// domain geometry has a group (elp_group.h) with its own stream, and every
+// group ticks on its own: a tick is `quantum` steps of all its members, and
+// when a group's tick ends the scheduler thread does its bookkeeping, admits
+// queued jobs whose device memory fits the HBM budget, retires finished ones
+// and launches its next tick at once -- no group waits for another, so a
+// small latency-bound melt never holds up the GPU.  Lattices stay resident
+// between dumps.  At a dump the job's state is copied device-to-device on
+// the group's stream at the end of the tick; I/O threads, each with its own
+// stream and scratch, rebuild the rings from the copy, check the final state
+// and format the TUV text while the group keeps computing.  A job follows
+// the same trajectory alone, in any mix, or through the single-melt API: its
+// kernel, counters and geometry depend only on its spec.
 //
 // The reference runs one fixed job per process (gpupol2/gpupol2.c:14-70 with
 // a synchronous dump per interval, gpupol2/gpupol_cuda.cu:52-76); it has no
@@ -73,25 +75,20 @@ struct Snap {
     SJob* job = nullptr;
     int64_t step = 0;
     bool final = false;
-    uint32_t* d_lat = nullptr;
+    uint32_t* d_lat = nullptr;            // copy of the job's state at `step`
     uint32_t* d_rec = nullptr;
-};
-
-struct IOWork {
-    SJob* job;
-    int64_t step;
-    bool final;
-    std::vector<int32_t> start;
-    std::vector<uint8_t> bonds;
+    cudaEvent_t ready = nullptr;          // recorded after the copy on the group's stream
 };
 
 struct SGroup {
     std::tuple<int, int, int, int, int, int> key;
     elp_group G;
     cudaStream_t s = nullptr;
-    cudaEvent_t ev = nullptr;
-    std::vector<SJob*> members;
-    bool dirty = false;
+    cudaEvent_t ev = nullptr;             // end of the running tick
+    std::vector<SJob*> members;           // resident jobs, including ones admitted during a tick
+    std::vector<SJob*> running;           // the members of the running tick
+    bool dirty = false;                   // members changed since the job table was built
+    bool busy = false;                    // a tick is in flight
 };
 
 }  // namespace
@@ -103,8 +100,6 @@ struct elp_server {
     uint32_t* d_table = nullptr;
     uint32_t* d_err = nullptr;            // 64 groups x 4 words
     unsigned long long* d_acc = nullptr;  // accepted moves (all jobs together)
-    cudaStream_t side = nullptr;
-    elp_walk_bufs wb;
 
     std::mutex mu;
     std::condition_variable cv, cv_done;
@@ -121,11 +116,10 @@ struct elp_server {
 
     std::vector<std::unique_ptr<SGroup>> groups;
     std::vector<SJob*> resident;
-    std::vector<Snap> pending;            // snapshots taken at the end of the last tick
 
     std::mutex io_mu;
     std::condition_variable io_cv;
-    std::deque<IOWork*> io_q;
+    std::deque<Snap> io_q;
     std::vector<std::thread> io_threads;
     std::atomic<int> io_busy{0};
     std::thread sched;
@@ -136,36 +130,64 @@ struct elp_server {
     }
 };
 
+static void fail_job(elp_server* s, SJob* j, elp_status st, const char* msg);
+
+// One I/O thread: rebuilds the rings of snapshots on its own stream and
+// scratch, checks the final state of a job, writes its TUV text.
 static void io_worker(elp_server* s)
 {
+    cudaSetDevice(s->o.device);
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    elp_walk_bufs wb;
+    std::vector<int32_t> start;
+    std::vector<uint8_t> bonds;
     for (;;) {
-        IOWork* w = nullptr;
+        Snap sn;
         {
             std::unique_lock<std::mutex> lk(s->io_mu);
             s->io_cv.wait(lk, [&] { return s->io_stop.load() || !s->io_q.empty(); });
-            if (s->io_q.empty()) return;
-            w = s->io_q.front();
+            if (s->io_q.empty()) break;
+            sn = s->io_q.front();
             s->io_q.pop_front();
         }
-        SJob* j = w->job;
+        SJob* j = sn.job;
         const int L = j->g.L, N = j->spec.N, P = j->P;
+        start.resize((size_t)P * 3);
+        bonds.resize((size_t)P * N);
+        cudaStreamWaitEvent(st, sn.ready, 0);
+        elp_status rc = elp_fetch_rings(sn.d_lat, sn.d_rec, L, N, P, 0, &wb, start.data(), bonds.data(), st);
+        if (sn.final && rc == ELP_OK) {
+            int32_t code = -1;
+            if (elp_check_melt(sn.d_lat, sn.d_rec, L, N, P, 0, &wb, &code, st) == ELP_OK) j->integrity = code;
+        }
+        std::string err = rc == ELP_OK ? std::string() : std::string(elp_last_error());
+        cudaFreeAsync(sn.d_lat, st);
+        cudaFreeAsync(sn.d_rec, st);
+        cudaStreamSynchronize(st);
+        cudaEventDestroy(sn.ready);
+        if (rc != ELP_OK) {
+            if (sn.final) fail_job(s, j, rc, err.c_str());
+            s->io_busy--;
+            continue;
+        }
         if (!j->dir.empty()) {
             size_t len = 0;
-            elp_format_tuv(L, N, P, w->start.data(), w->bonds.data(), nullptr, 0, &len);
+            elp_format_tuv(L, N, P, start.data(), bonds.data(), nullptr, 0, &len);
             std::string text(len + 1, '\0');
-            elp_format_tuv(L, N, P, w->start.data(), w->bonds.data(), &text[0], len + 1, &len);
+            elp_format_tuv(L, N, P, start.data(), bonds.data(), &text[0], len + 1, &len);
             char path[4096];
-            snprintf(path, sizeof(path), "%s/t=%lld_dev=0.res", j->dir.c_str(), (long long)w->step);
+            snprintf(path, sizeof(path), "%s/t=%lld_dev=0.res", j->dir.c_str(), (long long)sn.step);
             FILE* f = fopen(path, "wb");
             if (f) {
                 fwrite(text.data(), 1, len, f);
                 fclose(f);
             }
         }
-        if (w->final) {
+        if (sn.final) {
             uint64_t h = 0xcbf29ce484222325ULL;
-            h = fnv1a(h, w->start.data(), w->start.size() * sizeof(int32_t));
-            h = fnv1a(h, w->bonds.data(), w->bonds.size());
+            h = fnv1a(h, start.data(), start.size() * sizeof(int32_t));
+            h = fnv1a(h, bonds.data(), bonds.size());
             j->checksum = h;
             std::lock_guard<std::mutex> lk(s->mu);
             j->t_done = s->now();
@@ -173,9 +195,10 @@ static void io_worker(elp_server* s)
             s->completed++;
             s->cv_done.notify_all();
         }
-        delete w;
         s->io_busy--;
     }
+    elp_walk_bufs_free(&wb);
+    cudaStreamDestroy(st);
 }
 
 static SGroup* group_for(elp_server* s, SJob* j)
@@ -191,7 +214,9 @@ static SGroup* group_for(elp_server* s, SJob* j)
     if (elp_group_init(&gp->G, j->g, s->nsm, 0, s->o.quantum, s->d_table, s->d_err + 4 * s->groups.size(), gp->s) !=
         cudaSuccess)
         return nullptr;
-    gp->G.graph_steps = s->o.quantum;
+    // membership changes every few ticks: a captured graph would be rebuilt
+    // about as often as it is replayed, so tiled groups launch directly
+    gp->G.use_graph = 0;
     s->groups.push_back(std::move(gp));
     return s->groups.back().get();
 }
@@ -253,6 +278,7 @@ static bool admit(elp_server* s)
             s->bytes_in_use += j->bytes;
         }
         j->t_start = s->now();
+        std::lock_guard<std::mutex> lk(s->mu);
         s->resident.push_back(j);
     }
 }
@@ -274,36 +300,72 @@ static bool rebuild(elp_server* s, SGroup* gp)
     return elp_group_commit(&G) == cudaSuccess;
 }
 
-// Rebuild rings of a snapshot on the side stream and hand them to I/O.
-static bool drain_snap(elp_server* s, Snap& sn)
+// End of a group's tick: count the steps of the jobs that ran, copy the
+// state of jobs that dump or finish (on the group's stream, before its next
+// tick) and hand the copies to the I/O threads, retire finished jobs.
+static bool complete_tick(elp_server* s, SGroup* gp, size_t gi)
 {
-    SJob* j = sn.job;
-    IOWork* w = new IOWork();
-    w->job = j;
-    w->step = sn.step;
-    w->final = sn.final;
-    w->start.resize((size_t)j->P * 3);
-    w->bonds.resize((size_t)j->P * j->spec.N);
-    elp_status st = elp_fetch_rings(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, 0, &s->wb, w->start.data(),
-                                    w->bonds.data(), s->side);
-    if (sn.final && st == ELP_OK) {
-        int32_t code = -1;
-        if (elp_check_melt(sn.d_lat, sn.d_rec, j->g.L, j->spec.N, j->P, 0, &s->wb, &code, s->side) == ELP_OK)
-            j->integrity = code;
+    const int64_t Q = s->o.quantum;
+    std::vector<SJob*> done;
+    for (SJob* j : gp->running) {
+        j->done_steps += Q;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->moves_done += (double)Q * j->spec.N * j->P;
+        }
+        const bool fin = j->done_steps >= j->nsteps;
+        const bool dump = j->dump_interval > 0 && j->done_steps % j->dump_interval == 0;
+        if (dump || fin) {
+            Snap sn;
+            sn.job = j;
+            sn.step = j->done_steps;
+            sn.final = fin;
+            const size_t S = (size_t)j->g.L * j->g.L * j->g.L;
+            if (cudaMallocAsync((void**)&sn.d_lat, S * 4, gp->s) != cudaSuccess ||
+                cudaMallocAsync((void**)&sn.d_rec, (size_t)j->P * ELP_REC_WORDS * 4, gp->s) != cudaSuccess ||
+                cudaEventCreateWithFlags(&sn.ready, cudaEventDisableTiming) != cudaSuccess) {
+                s->fatal = ELP_ERR_NOMEM;
+                s->fatal_msg = "snapshot allocation failed";
+                return false;
+            }
+            cudaMemcpyAsync(sn.d_lat, j->lat, S * 4, cudaMemcpyDeviceToDevice, gp->s);
+            cudaMemcpyAsync(sn.d_rec, j->rec, (size_t)j->P * ELP_REC_WORDS * 4, cudaMemcpyDeviceToDevice, gp->s);
+            cudaEventRecord(sn.ready, gp->s);
+            if (dump) j->dumps++;
+            s->io_busy++;
+            {
+                std::lock_guard<std::mutex> lk(s->io_mu);
+                s->io_q.push_back(sn);
+            }
+            s->io_cv.notify_one();
+        }
+        if (fin) done.push_back(j);
     }
-    cudaFreeAsync(sn.d_lat, s->side);
-    cudaFreeAsync(sn.d_rec, s->side);
-    if (st != ELP_OK) {
-        delete w;
-        if (sn.final) fail_job(s, j, st, elp_last_error());
-        return cudaStreamSynchronize(s->side) == cudaSuccess;
+    for (SJob* j : done) {
+        cudaFreeAsync(j->lat, gp->s);
+        cudaFreeAsync(j->rec, gp->s);
+        for (size_t i = 0; i < gp->members.size(); i++)
+            if (gp->members[i] == j) {
+                gp->members.erase(gp->members.begin() + (long)i);
+                break;
+            }
+        gp->dirty = true;
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->bytes_in_use -= j->bytes;
     }
-    s->io_busy++;
-    {
-        std::lock_guard<std::mutex> lk(s->io_mu);
-        s->io_q.push_back(w);
+    gp->running.clear();
+    // a domain whose monomer-0 runs outgrew its label table stops the server
+    uint32_t flag = 0;
+    if (cudaMemcpy(&flag, s->d_err + 4 * gi, sizeof(flag), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        s->fatal = ELP_ERR_CUDA;
+        s->fatal_msg = "cannot read device error flags";
+        return false;
     }
-    s->io_cv.notify_one();
+    if (flag) {
+        s->fatal = ELP_ERR_STATE;
+        s->fatal_msg = "a domain held more monomer-0 runs than its label table";
+        return false;
+    }
     return true;
 }
 
@@ -313,104 +375,57 @@ static void scheduler(elp_server* s)
     const int64_t Q = s->o.quantum;
     for (;;) {
         if (!admit(s)) break;
-        for (auto& gp : s->groups)
-            if (gp->dirty && !rebuild(s, gp.get())) {
+        bool active = false, progressed = false;
+        for (size_t gi = 0; gi < s->groups.size() && !s->fatal; gi++) {
+            SGroup* gp = s->groups[gi].get();
+            if (gp->busy) {
+                const cudaError_t q = cudaEventQuery(gp->ev);
+                if (q == cudaErrorNotReady) {
+                    active = true;
+                    continue;
+                }
+                gp->busy = false;
+                progressed = true;
+                if (q != cudaSuccess) {
+                    s->fatal = ELP_ERR_CUDA;
+                    s->fatal_msg = "tick failed";
+                    break;
+                }
+                if (!complete_tick(s, gp, gi)) break;
+            }
+            if (gp->members.empty()) continue;
+            if (gp->dirty && !rebuild(s, gp)) {
                 s->fatal = ELP_ERR_CUDA;
                 s->fatal_msg = "group rebuild failed";
+                break;
             }
-        if (s->fatal) break;
-        // one tick on every group with members
-        bool any = false;
-        for (auto& gp : s->groups) {
-            if (gp->members.empty()) continue;
-            any = true;
+            gp->running = gp->members;
             if (elp_group_run(&gp->G, Q) != cudaSuccess || cudaEventRecord(gp->ev, gp->s) != cudaSuccess) {
                 s->fatal = ELP_ERR_CUDA;
                 s->fatal_msg = "launch failed";
+                break;
             }
+            gp->busy = true;
+            active = progressed = true;
         }
-        // while the tick computes: finish the snapshots of the previous tick
-        for (Snap& sn : s->pending)
-            if (!drain_snap(s, sn)) {
-                s->fatal = ELP_ERR_CUDA;
-                s->fatal_msg = "snapshot failed";
-            }
-        s->pending.clear();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->resident.clear();
+            for (auto& gp : s->groups)
+                for (SJob* j : gp->members) s->resident.push_back(j);
+        }
         if (s->fatal) break;
-        if (!any) {
+        if (!active) {
             std::unique_lock<std::mutex> lk(s->mu);
             if (s->stop.load() && s->queue.empty()) break;
             s->cv.wait_for(lk, std::chrono::milliseconds(2));
             continue;
         }
-        // tick done: bookkeeping, snapshots, retirements
-        std::vector<SJob*> keep;
-        for (auto& gp : s->groups) {
-            if (gp->members.empty()) continue;
-            if (cudaEventSynchronize(gp->ev) != cudaSuccess) {
-                s->fatal = ELP_ERR_CUDA;
-                s->fatal_msg = "tick failed";
-                break;
-            }
-            std::vector<SJob*> stay;
-            for (SJob* j : gp->members) {
-                j->done_steps += Q;
-                const bool fin = j->done_steps >= j->nsteps;
-                const bool dump = j->dump_interval > 0 && j->done_steps % j->dump_interval == 0;
-                {
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    s->moves_done += (double)Q * j->spec.N * j->P;
-                }
-                if (dump || fin) {
-                    Snap sn;
-                    sn.job = j;
-                    sn.step = j->done_steps;
-                    sn.final = fin;
-                    const size_t S = (size_t)j->g.L * j->g.L * j->g.L;
-                    if (cudaMallocAsync((void**)&sn.d_lat, S * 4, gp->s) != cudaSuccess ||
-                        cudaMallocAsync((void**)&sn.d_rec, (size_t)j->P * ELP_REC_WORDS * 4, gp->s) != cudaSuccess) {
-                        s->fatal = ELP_ERR_NOMEM;
-                        s->fatal_msg = "snapshot allocation failed";
-                        break;
-                    }
-                    cudaMemcpyAsync(sn.d_lat, j->lat, S * 4, cudaMemcpyDeviceToDevice, gp->s);
-                    cudaMemcpyAsync(sn.d_rec, j->rec, (size_t)j->P * ELP_REC_WORDS * 4, cudaMemcpyDeviceToDevice, gp->s);
-                    if (dump) j->dumps++;
-                    s->pending.push_back(sn);
-                }
-                if (fin) {
-                    cudaFreeAsync(j->lat, gp->s);
-                    cudaFreeAsync(j->rec, gp->s);
-                    std::lock_guard<std::mutex> lk(s->mu);
-                    s->bytes_in_use -= j->bytes;
-                    gp->dirty = true;
-                } else {
-                    stay.push_back(j);
-                }
-            }
-            gp->members.swap(stay);
-            // snapshot copies must land before the side stream reads them
-            cudaEventRecord(gp->ev, gp->s);
-            cudaStreamWaitEvent(s->side, gp->ev, 0);
-        }
-        s->resident.clear();
-        for (auto& gp : s->groups)
-            for (SJob* j : gp->members) s->resident.push_back(j);
-        uint32_t flags[64 * 4];
-        if (cudaMemcpy(flags, s->d_err, sizeof(flags), cudaMemcpyDeviceToHost) != cudaSuccess) {
-            s->fatal = ELP_ERR_CUDA;
-            s->fatal_msg = "cannot read device error flags";
-        }
-        for (size_t g = 0; g < s->groups.size() && !s->fatal; g++)
-            if (flags[4 * g]) {
-                s->fatal = ELP_ERR_STATE;
-                s->fatal_msg = "a domain held more monomer-0 runs than its label table";
-            }
-        if (s->fatal) break;
+        if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
-    for (Snap& sn : s->pending) drain_snap(s, sn);
-    s->pending.clear();
-    cudaStreamSynchronize(s->side);
+    // let the last ticks end before the jobs are failed or the groups freed
+    for (auto& gp : s->groups)
+        if (gp->busy) cudaEventSynchronize(gp->ev);
     if (s->fatal) {
         std::lock_guard<std::mutex> lk(s->mu);
         for (SJob* j : s->resident) {
@@ -464,8 +479,7 @@ extern "C" elp_status elp_server_create(const elp_server_opts* opts, elp_server*
     if (cudaMalloc((void**)&s->d_table, 4096) != cudaSuccess || cudaMalloc((void**)&s->d_err, 64 * 16) != cudaSuccess ||
         cudaMalloc((void**)&s->d_acc, 8) != cudaSuccess ||
         cudaMemcpy(s->d_table, tab, 4096, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(s->d_err, 0, 64 * 16) != cudaSuccess || cudaMemset(s->d_acc, 0, 8) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaMemset(s->d_err, 0, 64 * 16) != cudaSuccess || cudaMemset(s->d_acc, 0, 8) != cudaSuccess) {
         cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc);
         delete s;
         return elp_fail(ELP_ERR_CUDA, "server set-up failed");
@@ -606,8 +620,6 @@ extern "C" void elp_server_destroy(elp_server* s)
         cudaStreamDestroy(gp->s);
         cudaEventDestroy(gp->ev);
     }
-    elp_walk_bufs_free(&s->wb);
-    cudaStreamDestroy(s->side);
     cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc);
     for (SJob* j : s->finished) delete j;
     delete s;
