@@ -46,7 +46,7 @@ typedef struct elp_ctx elp_ctx;
 
 typedef struct elp_job_spec {
     int32_t L;                /* cubic box edge (sites) */
-    int32_t N;                /* monomers per ring */
+    int32_t N;                /* monomers per ring, 3 .. 65536 (linear chains: .. 65535) */
     int32_t P;                /* rings; <= 0: round(density * L^3 / N) as GetNPol */
     double density;           /* monomers per site, used when P <= 0 */
     uint32_t seed;            /* Philox key word 0 */

@@ -92,6 +92,9 @@ elp_status elp_resolve_spec(const elp_job_spec* spec, int* P, elp_geometry* g)
     if (spec->linear != 0 && spec->linear != 1) return elp_fail(ELP_ERR_ARG, "linear must be 0 or 1");
     if (spec->linear && spec->kernel == 1)
         return elp_fail(ELP_ERR_ARG, "linear chains run on the specialised kernels only");
+    // run lengths are 16-bit: a ring spans two sites at least, a linear chain may sit on one
+    if (spec->linear && spec->N > ELP_MAX_N - 1)
+        return elp_fail(ELP_ERR_ARG, "linear chain length N=%d above %d", spec->N, ELP_MAX_N - 1);
     if (spec->N < 3 || spec->N > ELP_MAX_N)
         return elp_fail(ELP_ERR_ARG, "ring length N=%d outside [3,%d]", spec->N, ELP_MAX_N);
     int p = spec->P > 0 ? spec->P : elp_get_npol(spec->density, spec->N, (long)spec->L * spec->L * spec->L);

@@ -235,7 +235,10 @@ int elp_initial_grid(int L, int N, int P, int* delta_out, int* nt_out, int* nv_o
         long ntot = (long)(L / delta) * (L / delta) * (L / (delta + 1));
         if (ntot < P) { delta--; break; }
     }
-    if (delta < 1 || delta >= L) return 1;
+    // every spacing fits (a handful of chains): the reference's loop runs out
+    // here and divides by zero; take the widest spacing, L - 1
+    if (delta >= L) delta = L - 1;
+    if (delta < 1) return 1;
     int nt = L / delta, nv = L / (delta + 1);
     if ((long)nt * nv * (L / delta) < P) return 1;
     *delta_out = delta;
