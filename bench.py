@@ -7,9 +7,11 @@ reference efpol's unit, cpupol/efpol_lib.c:123) of the workload.
 
 Default workload: the single large ring melt L=128, N=1000, density 1.2
 (2517 rings), seed 7, initialised like the reference's CreatePolymers
-(synthetic: no dataset exists for this path).  The lattice (8 MB) is smaller
-than L2, so L2 is flushed between timed steps (a 256 MB write outside the
-timed events).  Extra legs on rank 0: the L=256, N=5000 melt (roofline
+(synthetic: no dataset exists for this path).  The melt runs --spl steps per
+kernel launch (a cooperative launch whose CTAs meet at a grid barrier between
+steps; the same bits as one step per launch).  The lattice (8 MB) is smaller
+than L2, so L2 is flushed before every timed launch (a 256 MB write outside
+the timed events).  Extra legs on rank 0: the L=256, N=5000 melt (roofline
 configuration), the reference CPU efpol timed on this host, and the
 end-to-end path through the C ABI with host buffers.
 
@@ -58,12 +60,13 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic(name):
-    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+def profile_traffic(name, spl):
+    """DRAM bytes per sweep launch of `spl` steps from the committed ncu
+    summary, if one was captured for that launch shape."""
     p = os.path.join(REPO, "profiles", "traffic.json")
     try:
         with open(p) as f:
-            return json.load(f).get(name)
+            return json.load(f).get(f"{name}/spl{spl}")
     except Exception:
         return None
 
@@ -189,7 +192,8 @@ def run_elp(args, rank, world):
     M = w["N"] * npol(w)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
-    m = elp.Melt(L=w["L"], N=w["N"], seed=replica_seed(w, rank), device=dev)
+    spl = max(1, args.spl)
+    m = elp.Melt(L=w["L"], N=w["N"], seed=replica_seed(w, rank), device=dev, steps_per_launch=spl)
     m.init_melt()
     m.run(args.warmup)
     m.sync()
@@ -197,7 +201,7 @@ def run_elp(args, rank, world):
 
     barrier(world)
     with ClockSampler(dev) as clk:
-        times = timed_steps(m, torch, flush, dev, args.steps)
+        times = timed_steps(m, torch, flush, dev, args.steps, spl)
     total_ms = max_over_ranks(sum(times), world)
     barrier(world)
     value = world * args.steps * M / (total_ms / 1e3)
@@ -206,23 +210,25 @@ def run_elp(args, rank, world):
 
     peak, peak_kind = measured_peak()
     achieved = algo_bytes(w) / (ms_per_step / 1e3) / 1e9
-    tr = profile_traffic(args.workload)
+    tr = profile_traffic(args.workload, spl)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference CreatePolymers initial melt)",
         "config": {"workload": f"ring melt L={w['L']} N={w['N']} density={w['density']} P={npol(w)} "
-                               f"seed={w['seed']}, one sweep kernel per step",
+                               f"seed={w['seed']}, {spl} steps per sweep launch",
+                   "steps_per_launch": spl,
                    "L": w["L"], "N": w["N"], "P": npol(w), "sites": w["L"] ** 3, "monomers": M,
                    "geometry": {"periodic": info.periodic, "tile": list(info.tile), "ncol": info.ncol,
                                 "domains": info.domains, "threads": info.threads},
-                   "l2": "flushed between timed steps (256 MB write on the melt's stream, queued before the start event)",
+                   "l2": f"flushed before every timed launch of {spl} steps (256 MB write on the melt's stream, "
+                         "queued before the start event); inside a launch the lattice stays in L2 between steps",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": algo_bytes(w),
+                     "algorithmic_bytes_per_launch": spl * algo_bytes(w),
                      "traffic": tr},
-        "gpu_launches": args.steps,
+        "gpu_launches": len(times),
     }
     clk_s = clk.summary()
     if clk_s:
@@ -248,7 +254,7 @@ def e2e_leg(elp, w, dev, args):
 
     interval = args.e2e_interval
     P, N = npol(w), w["N"]
-    m = elp.Melt(L=w["L"], N=N, seed=w["seed"], device=dev)
+    m = elp.Melt(L=w["L"], N=N, seed=w["seed"], device=dev, steps_per_launch=max(1, args.spl))
     m.init_melt()
     m.run(args.warmup)
     start_t = torch.empty((P, 3), dtype=torch.int32).pin_memory()
@@ -278,18 +284,22 @@ def e2e_leg(elp, w, dev, args):
             "path": "elp_load_chains(host) + elp_run(interval) + elp_fetch_chains(host), wall clock"}
 
 
-def timed_steps(m, torch, flush, dev, nsteps):
-    """Per step: flush L2 (a 256 MB write) on the melt's own stream, then one
-    MC step between CUDA events on that stream.  The flush is queued ahead of
-    the start event, so the events see the sweep launch alone and the host's
-    launch latency hides behind the flush."""
+def timed_steps(m, torch, flush, dev, nsteps, spl=1):
+    """nsteps MC steps in launches of spl steps.  Per launch: flush L2 (a
+    256 MB write) on the melt's own stream, then the launch between CUDA
+    events on that stream.  The flush is queued ahead of the start event, so
+    the events see the sweep launch alone and the host's launch latency hides
+    behind the flush.  Returns the time of each launch (ms)."""
     s = torch.cuda.ExternalStream(m.stream_ptr(), device=f"cuda:{dev}")
     torch.cuda.synchronize()
     times = []
-    for _ in range(nsteps):
+    done = 0
+    while done < nsteps:
+        k = min(spl, nsteps - done)
         with torch.cuda.stream(s):
             flush.fill_(1.0)
-        times.append(m.run_timed(1))
+        times.append(m.run_timed(k))
+        done += k
     torch.cuda.synchronize()
     return times
 
@@ -297,18 +307,21 @@ def timed_steps(m, torch, flush, dev, nsteps):
 def l256_leg(elp, torch, dev, flush, args):
     w = WORKLOADS["L256"]
     M = w["N"] * npol(w)
-    m = elp.Melt(L=w["L"], N=w["N"], seed=w["seed"], device=dev)
+    spl = max(1, args.l256_spl)
+    m = elp.Melt(L=w["L"], N=w["N"], seed=w["seed"], device=dev, steps_per_launch=spl)
     m.init_melt()
-    m.run(3)
+    m.run(3 * spl)
     m.sync()
-    times = timed_steps(m, torch, flush, dev, max(3, args.steps // 2))
-    ms = sum(times) / len(times)
+    nsteps = max(3 * spl, args.steps // 2 // spl * spl)
+    times = timed_steps(m, torch, flush, dev, nsteps, spl)
+    ms = sum(times) / nsteps
     peak, _ = measured_peak()
     achieved = algo_bytes(w) / (ms / 1e3) / 1e9
-    return {"workload": "ring melt L=256 N=5000 P=4027 seed=11", "value": M / (ms / 1e3), "unit": UNIT,
-            "ms_per_step": ms,
+    return {"workload": f"ring melt L=256 N=5000 P=4027 seed=11, {spl} steps per sweep launch", "value": M / (ms / 1e3),
+            "unit": UNIT, "ms_per_step": ms, "steps": nsteps, "steps_per_launch": spl,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "algorithmic_bytes_per_launch": algo_bytes(w), "traffic": profile_traffic("L256")}}
+                         "algorithmic_bytes_per_launch": spl * algo_bytes(w),
+                         "traffic": profile_traffic("L256", spl)}}
 
 
 # ---- batched ensemble (512 replicas) ------------------------------------------
@@ -375,8 +388,10 @@ def batched_leg(elp, dev, args):
         m.close()
     plain = moves * args.batch_steps / (pms / 1e3)
     b.close()
+    # tiled groups take one step per launch inside a batch of several groups
     geoms = {str(L): {"periodic": t["periodic"], "tile": list(t["tile"]), "ncol": t["ncol"],
-                      "steps_per_launch": t["steps_per_launch"]} for L, t in tuned.items()}
+                      "steps_per_launch": t["steps_per_launch"] if t["periodic"] == 1 else 1}
+             for L, t in tuned.items()}
     return {"workload": f"{len(specs)} ring melts, L uniform on {{16,24,32,48,64}}, N log-uniform on [50,1000], "
                         f"density 1.2, seeds 1000..{999 + len(specs)}",
             "monomers": moves, "steps": args.batch_steps, "warmup": args.batch_warmup,
@@ -473,6 +488,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="elp", choices=["elp", "reference"])
     ap.add_argument("--workload", default="L128", choices=sorted(WORKLOADS))
+    ap.add_argument("--spl", type=int, default=20, help="MC steps per sweep launch (headline workload and e2e)")
+    ap.add_argument("--l256-spl", type=int, default=10, help="MC steps per sweep launch of the L=256 leg")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--ref-steps", type=int, default=8)
     ap.add_argument("--e2e-interval", type=int, default=100)

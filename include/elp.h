@@ -55,7 +55,8 @@ typedef struct elp_job_spec {
     int32_t tile[3];          /* tiled domain edges, 0 = auto */
     int32_t ncol;             /* colour modulus, 0 = auto */
     int32_t device;           /* CUDA device ordinal */
-    int32_t steps_per_launch; /* whole-box domains: steps per kernel launch (>=1) */
+    int32_t steps_per_launch; /* steps per kernel launch (>=1); tiled domains: a cooperative launch with a
+                                 grid barrier between steps.  Any value gives the same bits. */
     int32_t kernel;           /* 0 auto (specialised when the shape has one), 1 generic */
     int32_t linear;           /* 0 ring polymers (efpol_ring), 1 linear chains (efpol_lin): the last
                                * bond of every chain is the end marker 0xf ('f' in TUV files).
@@ -224,9 +225,12 @@ const char* elp_last_error(void);
  * size and ring length advanced together on one GPU.  All lattices live in
  * one packed arena; melts with the same domain geometry share one kernel
  * launch and a stream, and groups of different shapes run concurrently.
- * Whole-box melts (L <= 32) run `steps_per_launch` steps per launch on chip;
- * tiled melts run one step per launch, replayed from a CUDA graph.  A melt
- * gives the same bits in a batch as alone with the same spec.
+ * Melts run `steps_per_launch` steps per launch: whole-box melts (L <= 32)
+ * on chip, tiled melts as one cooperative launch whose CTAs meet at a grid
+ * barrier between steps (in a batch of more than one group, tiled groups take
+ * one step per launch, so that groups keep overlapping); tiled launches are
+ * replayed from a CUDA graph.  A melt gives the same bits in a batch as alone
+ * with the same spec, whatever its steps per launch.
  * The reference has no batched engine; its nearest form is one independent
  * replica per GPU (gpupol2/gpupol_init.c:8-33, gpupol2/gpupol_cuda.cu:129-146). */
 typedef struct elp_batch elp_batch;
@@ -253,8 +257,8 @@ elp_status elp_batch_job_info(const elp_batch* b, int32_t job, elp_info* info);
 void elp_batch_destroy(elp_batch* b);
 
 /* Autotuner: times the candidate domain geometries of `in` -- the whole box
- * on chip (with 1, 10 or 100 steps per launch) and every tile shape that
- * divides the box -- on `copies` copies of its initial melt run as one batch
+ * on chip and every tile shape that divides the box, each with 1, 10 or 100
+ * steps per launch -- on `copies` copies of its initial melt run as one batch
  * for `steps` steps, and returns the fastest as an explicit spec (periodic,
  * tile, ncol, steps_per_launch filled in).  Whole-box domains have no tile
  * walls, so a tiled shape is chosen only when it is over 1.5x faster.  The tile shape is part of a

@@ -103,7 +103,7 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
         mm.linear = specs[j].linear;
         mm.seed = specs[j].seed;
         mm.salt = specs[j].salt;
-        const int spl = mm.g.periodic ? (specs[j].steps_per_launch > 0 ? specs[j].steps_per_launch : 1) : 1;
+        const int spl = specs[j].steps_per_launch > 0 ? specs[j].steps_per_launch : 1;
         const int gen = specs[j].kernel == 1;
         // rings and linear chains run in different groups (different kernels)
         auto key = std::make_tuple(mm.g.periodic, mm.g.L, mm.g.tx, mm.g.ty, mm.g.tz, mm.g.ncol, spl, gen, mm.linear);
@@ -117,6 +117,13 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
         lat_words += ((size_t)mm.g.L * mm.g.L * mm.g.L + 63) / 64 * 64;
         rec_words += (size_t)mm.P * ELP_REC_WORDS;
     }
+    // A tiled launch of several steps is cooperative: it starts only when all
+    // its CTAs fit at once and then holds every SM until its last step, which
+    // would serialise the groups that otherwise overlap.  With more than one
+    // group, tiled groups take one step per launch (the same bits).
+    if (gdesc.size() > 1)
+        for (auto& gd : gdesc)
+            if (!std::get<0>(gd).periodic) std::get<1>(gd) = 1;
     // one packed arena for all lattices and records
     e = cudaMalloc((void**)&b->d_lat, lat_words * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_rec, rec_words * 4);
@@ -374,9 +381,9 @@ extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info
 }
 
 // ---- autotuner ---------------------------------------------------------------
-// Candidate geometries for a melt: its whole box on chip (if that fits) with a
-// few steps-per-launch values, and every tile shape of the preference list
-// that divides the box.  Each is timed on `copies` copies of the initial melt
+// Candidate geometries for a melt: its whole box on chip (if that fits) and
+// every tile shape of the preference list that divides the box, each with a
+// few steps-per-launch values.  Each is timed on `copies` copies of the initial melt
 // run as one batch (the best tile depends on how many melts share the GPU).
 extern "C" elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32_t steps, elp_job_spec* out,
                                    float* ms_per_step)
@@ -406,12 +413,16 @@ extern "C" elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32
         s.periodic = 0;
         s.tile[0] = t[0]; s.tile[1] = t[1]; s.tile[2] = t[2];
         s.ncol = 0;
-        s.steps_per_launch = 1;
         int P;
         elp_geometry g;
         if (in->L % t[0] || in->L % t[1] || in->L % t[2]) continue;
         if (elp_resolve_spec(&s, &P, &g) != ELP_OK) continue;
-        cand.push_back(s);
+        const int spls[] = {1, 10, 100};
+        for (int spl : spls) {
+            if (spl > steps) continue;
+            s.steps_per_launch = spl;
+            cand.push_back(s);
+        }
     }
     if (cand.empty()) return elp_fail(ELP_ERR_ARG, "no candidate geometry for L=%d", in->L);
     float best = -1.f, best_score = 0.f;

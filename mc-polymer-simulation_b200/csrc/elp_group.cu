@@ -34,6 +34,7 @@ Sweep2Launch make_launch(const elp_group* G, int nsteps, uint32_t step_base, int
     l.args.step_dev = G->d_ctr;
     l.args.table = G->d_table;
     l.args.error = G->d_error;
+    l.args.grid_bar = G->d_ctr + 1;
     return l;
 }
 
@@ -89,9 +90,10 @@ cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int 
     G->stream = stream;
     G->d_table = d_table;
     G->d_error = d_error;
-    cudaError_t e = cudaMalloc((void**)&G->d_ctr, sizeof(uint32_t));
+    // step counter and the two counts of the grid barrier of tiled launches
+    cudaError_t e = cudaMalloc((void**)&G->d_ctr, 4 * sizeof(uint32_t));
     if (e != cudaSuccess) return e;
-    return cudaMemsetAsync(G->d_ctr, 0, sizeof(uint32_t), stream);
+    return cudaMemsetAsync(G->d_ctr, 0, 4 * sizeof(uint32_t), stream);
 }
 
 void elp_group_add(elp_group* G, uint32_t* lat, uint32_t* rec, unsigned long long* acc, int N, int nchains,
@@ -188,35 +190,40 @@ cudaError_t elp_group_run(elp_group* G, int64_t nsteps)
         }
         return cudaSuccess;
     }
-    if (G->specialised && G->use_graph && nsteps >= G->graph_steps) {
+    // tiled domains: the specialised kernel takes spl steps per (cooperative)
+    // launch, the generic one a single step
+    const int k = G->specialised ? G->spl : 1;
+    const int gsteps = G->graph_steps > k ? G->graph_steps / k * k : k;
+    if (G->specialised && G->use_graph && nsteps >= gsteps) {
         const uint32_t base = (uint32_t)(G->steps_done - G->ctr_mirror);
         if (!G->graph || G->graph_base != base) {
             if (G->graph) cudaGraphExecDestroy(G->graph);
             G->graph = nullptr;
             cudaGraph_t gr;
             if ((e = cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-            for (int i = 0; i < G->graph_steps; i++) {
-                Sweep2Launch l = make_launch(G, 1, base + (uint32_t)i, 0);
+            for (int i = 0; i < gsteps; i += k) {
+                Sweep2Launch l = make_launch(G, k, base + (uint32_t)i, 0);
                 elp_launch_sweep2(&l, G->stream);
             }
-            ctr_add_kernel<<<1, 1, 0, G->stream>>>(G->d_ctr, (uint32_t)G->graph_steps);
+            ctr_add_kernel<<<1, 1, 0, G->stream>>>(G->d_ctr, (uint32_t)gsteps);
             if ((e = cudaStreamEndCapture(G->stream, &gr)) != cudaSuccess) return e;
             e = cudaGraphInstantiate(&G->graph, gr, 0);
             cudaGraphDestroy(gr);
             if (e != cudaSuccess) return e;
             G->graph_base = base;
         }
-        while (nsteps >= G->graph_steps) {
+        while (nsteps >= gsteps) {
             if ((e = cudaGraphLaunch(G->graph, G->stream)) != cudaSuccess) return e;
-            G->steps_done += (uint64_t)G->graph_steps;
-            G->ctr_mirror += (uint32_t)G->graph_steps;
-            nsteps -= G->graph_steps;
+            G->steps_done += (uint64_t)gsteps;
+            G->ctr_mirror += (uint32_t)gsteps;
+            nsteps -= gsteps;
         }
     }
     while (nsteps > 0) {
-        if ((e = launch_once(G, 1, (uint32_t)(G->steps_done - G->ctr_mirror))) != cudaSuccess) return e;
-        G->steps_done += 1;
-        nsteps -= 1;
+        const int kk = (int)(nsteps < k ? nsteps : k);
+        if ((e = launch_once(G, kk, (uint32_t)(G->steps_done - G->ctr_mirror))) != cudaSuccess) return e;
+        G->steps_done += (uint64_t)kk;
+        nsteps -= kk;
     }
     return cudaSuccess;
 }

@@ -21,7 +21,7 @@ struct elp_group {
     int specialised;                  // a specialised kernel fits this group
     int threads;                      // block size of the sweep kernel in use
     size_t smem;                      // its dynamic shared memory per block
-    int spl;                          // whole-box domains: steps per launch
+    int spl;                          // steps per launch (tiled: specialised kernel only)
     int use_graph;                    // tiled domains: replay launches from a CUDA graph
     int graph_steps;                  // launches captured per graph
     cudaStream_t stream;

@@ -65,7 +65,7 @@ int elp_geometry_ok(const elp_geometry* g)
 
 // Worst shared-memory bank multiplicity of the first anchor load of a warp,
 // over all colours and warps.
-static int bank_cost(const elp_geometry* g, int ox, int sx, int sxy)
+static int bank_cost(const elp_geometry* g, int ox, int sx, int sxy, bool permuted)
 {
     int n = g->ncol, ty = g->ty, tz = g->tz;
     long R = (long)ty * tz, A = R * (g->tx / n), G = A / 4;
@@ -75,6 +75,10 @@ static int bank_cost(const elp_geometry* g, int ox, int sx, int sxy)
             int cnt[32] = {0};
             for (long g0 = w0; g0 < w0 + 32 && g0 < G; g0++) {
                 long j = g0 / R, row = g0 % R;
+                if (permuted) {  // lane -> row of an 8 x 4 block of rows
+                    const long lane = row & 31, w = row >> 5;
+                    row = (lane & 7) + 8 * (w % (ty / 8)) + (long)ty * ((lane >> 3) + 4 * (w / (ty / 8)));
+                }
                 int y = (int)(row % ty), z = (int)(row / ty);
                 int x = (((c - 2 * y - 3 * z) % n) + n) % n + n * (int)j;
                 long idx = ox + x + (long)sx * y + (long)sxy * z;
@@ -86,24 +90,37 @@ static int bank_cost(const elp_geometry* g, int ox, int sx, int sxy)
     return worst;
 }
 
+// Whole box: rows of L words (padded for banks).  Tiles: each row holds the
+// 16-byte aligned span of TX + 4 words that the tile copy fetches (the tile
+// at offset x0 mod 4 in it) and one halo word before it, so the row stride is
+// a multiple of 4 words and at least TX + 5; rows y = -1, TY and planes
+// z = -1, TZ are halo.  The specialised kernels hand out anchors to a warp's
+// threads from an 8 x 4 block of (y, z) rows where the tile allows
+// (`permuted`), which the bank score follows.
 static void layout_search(const elp_geometry* g, elp_smem_layout* lay)
 {
-    int halo = g->periodic ? 0 : 2;
+    const int per = g->periodic;
+    const long A = (long)g->ty * g->tz * (g->tx / g->ncol), R = (long)g->ty * g->tz;
+    // threads own one or two anchors in the tiled shapes: AT = A or A / 2
+    const bool permuted = !per && g->ty % 8 == 0 && g->tz % 4 == 0 && (A % R == 0) && ((A / 2) % R == 0 || A == R);
     int best_sx = 0, best_sxy = 0, best = 1 << 30;
+    const int sx0 = per ? g->tx : (g->tx + 5 + 3) & ~3;
     for (int px = 0; px < 8; px++) {
-        int sx = g->tx + halo + px;
+        int sx = per ? sx0 + px : sx0 + 4 * (px & 1);
+        if (!per && px > 1) break;
         for (int pz = 0; pz < 32; pz += 1) {
-            int sxy = sx * (g->ty + halo) + pz;
-            int ox = g->periodic ? 0 : 1 + sx + sxy;
-            int cost = bank_cost(g, ox, sx, sxy) * 64 + px + pz;  // prefer small padding
+            int sxy = per ? sx * g->ty + pz : sx * (g->ty + 2) + 4 * pz;
+            int ox = per ? 0 : sx + sxy + 4;
+            int cost = bank_cost(g, ox, sx, sxy, permuted) * 64 + px + pz;  // prefer small padding
             if (cost < best) { best = cost; best_sx = sx; best_sxy = sxy; }
         }
     }
     lay->sx = best_sx;
     lay->sxy = best_sxy;
-    lay->ox = g->periodic ? 0 : 1 + best_sx + best_sxy;
-    lay->words = best_sxy * (g->tz + halo);
-    lay->anchors = g->ty * g->tz * (g->tx / g->ncol);
+    lay->ox = per ? 0 : best_sx + best_sxy + 4;
+    lay->words = per ? best_sxy * g->tz
+                     : ((lay->ox + best_sx * g->ty + best_sxy * g->tz + g->tx + 4 + 3) & ~3);
+    lay->anchors = (int)A;
     lay->groups = lay->anchors / 4;
     lay->bytes = (size_t)lay->words * 4 + 4096 + 27 * 16 * 4 + 64 * 4;
 }

@@ -45,11 +45,12 @@ struct BatchLaunch {
     const BatchJob* jobs;          // device job table
     const uint2* items;            // device work items {job, domain}
     int nitems;
-    int nsteps;                    // steps per launch (whole-box domains only; else 1)
+    int nsteps;                    // steps per launch
     uint32_t step_base;            // added to every job's step0 ...
     const uint32_t* step_dev;      // ... and, if set, this device counter (graph replays)
     const uint32_t* table;         // 4096-byte transition table
     uint32_t* error;               // device error flags
+    uint32_t* grid_bar;            // tiled domains, nsteps > 1: {arrivals, exits}, zero between launches
 };
 
 #include "elp_internal.h"

@@ -215,8 +215,11 @@ static SGroup* group_for(elp_server* s, SJob* j)
         cudaSuccess)
         return nullptr;
     // membership changes every few ticks: a captured graph would be rebuilt
-    // about as often as it is replayed, so tiled groups launch directly
+    // about as often as it is replayed, so tiled groups launch directly, one
+    // step per launch (a launch of several tiled steps is cooperative and
+    // holds every SM it uses until its last step, stalling the other groups)
     gp->G.use_graph = 0;
+    if (!j->g.periodic) gp->G.spl = 1;
     s->groups.push_back(std::move(gp));
     return s->groups.back().get();
 }

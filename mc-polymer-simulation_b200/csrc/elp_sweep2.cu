@@ -11,8 +11,16 @@
 //     (bits 5-15) into a small shared-memory table {chain, offset, site};
 //     the chain records in global memory are read when the tile is loaded and
 //     written back when it is stored, so no move waits on global memory;
-//   * tiles are fetched with cp.async (4-byte granules: the origin shift
-//     makes rows unaligned) and the grid is persistent over the tiles.
+//   * a tile's rows are fetched by bulk copies (the TMA engine, one or two
+//     per row) that complete on a shared-memory mbarrier.  The origin shift
+//     makes a row start anywhere, so each copy takes the 16-byte aligned
+//     span around the row (TX + 4 words) and the tile sits sh = x0 mod 4
+//     words into it; the words of the span outside the tile become halo
+//     words.  Tiles go back with 16-byte stores (single words at the ragged
+//     ends).  Rows are 16-byte aligned in shared memory, and the threads of
+//     a warp take anchors from an 8 x 4 block of rows so that their first
+//     loads hit 32 different banks;
+//   * the grid is persistent over the tiles.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -26,7 +34,96 @@ __device__ __forceinline__ void cp_async4(uint32_t* sdst, const uint32_t* gsrc)
     uint32_t s = (uint32_t)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_async16(uint32_t* sdst, const uint32_t* gsrc)
+{
+    uint32_t s = (uint32_t)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// ---- bulk copies (TMA engine, untiled) completing on a shared-memory mbarrier
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// one arrival that also announces `bytes` of copies for the current phase
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* m, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* m, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for phase `parity` of the mbarrier to complete, giving up after
+// `limit` polls (each poll may itself suspend the thread for a while).
+__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, int limit)
+{
+    for (int i = 0; i < limit; i++)
+        if (mbar_test(m, parity)) return true;
+    return false;
+}
+// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(uint32_t* dst, const uint32_t* src, uint32_t bytes, uint64_t* m)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(m))
+                 : "memory");
+}
+// order this thread's earlier shared-memory accesses before later bulk copies
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+constexpr int MBAR_POLLS = 1 << 22;
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// order generic-proxy accesses to global memory with bulk copies
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+constexpr int GRID_POLLS = 1 << 24;
+
+// Barrier over all CTAs of a cooperative launch: each CTA adds one to
+// bar[0] and waits (bounded) until it reaches `target`.  The CTA's stores
+// before it are visible to every CTA's loads and bulk copies after it.
+// Returns false, in every thread of the CTA, when the wait gave up.
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t target)
+{
+    bool ok = true;
+    fence_proxy_async_global();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        for (int n = 0; ld_acquire_gpu(bar) < target; n++) {
+            if (n >= GRID_POLLS) { ok = false; break; }
+            __nanosleep(64);
+        }
+    }
+    const bool failed = __syncthreads_or(!ok) != 0;
+    fence_proxy_async_global();
+    return !failed;
+}
+// Last act of every CTA of a cooperative launch: the last one to leave
+// zeroes the barrier counts for the next launch on the stream.
+__device__ __forceinline__ void grid_exit(uint32_t* bar)
+{
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(bar + 1, 1u) == gridDim.x - 1) {
+        atomicExch(bar, 0u);
+        atomicExch(bar + 1, 0u);
+    }
+}
 
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K>
 struct Shape {
@@ -34,13 +131,20 @@ struct Shape {
     static constexpr int A = R * (TX / NC);   // anchors per substep
     static constexpr int G = A / 4;           // Philox counters per substep group
     static constexpr int AT = A / K;          // threads that own anchors
-    static constexpr int HALO = PER ? 0 : 2;
-    static constexpr int OX = PER ? 0 : 1 + SX + SXY;
-    static constexpr int WORDS = SXY * (TZ + HALO);
+    // Tiled domains: row y of plane z starts at OX + SX y + SXY z (16-byte
+    // aligned) and holds the copied span of TX + 4 words, the tile at offset
+    // sh in it; rows y = -1, TY and planes z = -1, TZ are halo, as is the
+    // word before each row (the previous row's padding).
+    static constexpr int SPAN = TX + 4;
+    static constexpr int OX = PER ? 0 : SX + SXY + 4;
+    static constexpr int WORDS = PER ? SXY * TZ : ((OX + SX * TY + SXY * TZ + SPAN + 3) & ~3);
     static constexpr int SITES = TX * TY * TZ;
+    // threads of a warp take anchors from an 8 x 4 block of (y, z) rows
+    static constexpr bool PERM = !PER && TY % 8 == 0 && TZ % 4 == 0 && AT % R == 0;
     // shared-memory word offsets: lattice, transition table (4096 bytes),
-    // neighbour offsets (27 x 16), colours, slot tables, slot count, and the
-    // Philox words of the current substep group when threads own < 4 anchors
+    // neighbour offsets (27 x 16), colours, slot tables, slot count, the
+    // Philox words of the current substep group when threads own < 4 anchors,
+    // and the mbarrier of the tile copies
     static constexpr int TABW = WORDS;
     static constexpr int OFFW = TABW + 1024;
     static constexpr int COLW = OFFW + 27 * 16;
@@ -50,8 +154,11 @@ struct Shape {
     static constexpr int NSLW = SSIW + CAP;
     static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
     static constexpr int RNDW = (HTABW + 64 + 4) & ~3;
-    static constexpr int TOTW = RNDW + (K < 4 ? 4 * G : 0);
+    static constexpr int MBW = RNDW + (K < 4 ? 4 * G : 0);
+    static constexpr int TOTW = MBW + 4;
     static constexpr size_t BYTES = (size_t)TOTW * 4;
+    static_assert(PER || (SX % 4 == 0 && SXY % 4 == 0 && SX >= SPAN + 1 && SXY >= SX * (TY + 2)),
+                  "tiled rows: 16-byte aligned, room for the span and the halo word before it");
 };
 
 constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
@@ -63,6 +170,25 @@ constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
 constexpr uint32_t HWALL = ELP_CUNIT | 3u;
 
 extern __shared__ __align__(16) uint32_t g_smem[];
+
+// A labelled word (global form: chain id in bits 5-31) entering shared
+// memory: claim a slot for the chain, keep {chain, offset, site} in the slot
+// table and put the slot number and the run length into the word.  Past the
+// table's capacity the word is left as it is (the overflow is reported
+// before the first substep).
+template <int CAP>
+__device__ __forceinline__ uint32_t take_slot(uint32_t wv, int idx, const uint32_t* rec, uint32_t* nslots,
+                                              uint32_t* slot_chain, uint32_t* slot_off, int* slot_site)
+{
+    const uint32_t slot = atomicAdd(nslots, 1u);
+    if (slot >= (uint32_t)CAP) return wv;
+    const uint32_t chain = wv >> 5;
+    const uint4 rr = __ldcg(reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)chain));
+    slot_chain[slot] = chain;
+    slot_off[slot] = rr.z;
+    slot_site[slot] = idx;
+    return (wv & 15) | ELP_LBIT | (slot << 5) | (rr.y << ELP_CSHIFT);
+}
 
 // The K anchors of one thread, one substep.  Returns accepted moves.
 // Anchor q takes its random byte at bit offset bsh[q] of the Philox word w.
@@ -264,11 +390,24 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     if (!PER)
         for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = HWALL;
 
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(g_smem + SH::MBW);
+    if (!PER && tid == 0) mbar_init(mbar, 1);
+    uint32_t mbar_phase = 0;
+
+    // Anchor an = g + q G of a substep takes byte q of Philox word g.  Thread
+    // tid owns anchors an = tid + q AT, or with PERM the anchors of the same
+    // x group whose row is the tid-th of the 8 x 4 row blocks.
     int base[K], rot[K], clsyz[K], xj[K], bsh[K], anq[K];
-    const int gq = tid % SH::G;   // Philox counter word 3 of this thread's anchors
+    int tperm = tid;
+    if (SH::PERM) {
+        const int r = tid % SH::R, lane = r & 31, w = r >> 5;
+        const int y = (lane & 7) + 8 * (w % (TY / 8)), z = (lane >> 3) + 4 * (w / (TY / 8));
+        tperm = tid - r + y + TY * z;
+    }
+    const int gq = tperm % SH::G;   // Philox counter word 3 of this thread's anchors
 #pragma unroll
     for (int q = 0; q < K; q++) {
-        int an = tid + q * SH::AT;
+        int an = tperm + q * SH::AT;
         anq[q] = an;
         bsh[q] = 8 * (an / SH::G);
         int j = an / SH::R, row = an % SH::R;
@@ -283,8 +422,19 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     }
     const bool active = tid < SH::AT;
     const uint32_t step_dev = a.step_dev ? *a.step_dev : 0u;
+    // Whole-box domains run their steps back to back on chip; tiled domains
+    // move their tiles every step, so a launch of several steps takes its
+    // steps one after another over all tiles, with a grid barrier between
+    // steps (the launch is cooperative: all CTAs are resident).
+    const int outer = PER ? 1 : a.nsteps, inner = PER ? a.nsteps : 1;
+    bool abort = false;
 
-    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
+    for (int so = 0; so < outer && !abort; so++) {
+    if (so > 0 && !grid_barrier(a.grid_bar, gridDim.x * (uint32_t)so)) {
+        if (tid == 0) atomicOr(a.error, 4u);
+        break;
+    }
+    for (int it = blockIdx.x; it < a.nitems && !abort; it += gridDim.x) {
         const uint2 item = a.items[it];
         const BatchJob& J = a.jobs[item.x];
         const int d = (int)item.y;
@@ -301,9 +451,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         D.x0 = 0; D.y0 = 0; D.z0 = 0;
         int accepted = 0;
         bool overflow = false;
+        int bse[K];   // anchor base indices of this tile (plus its offset sh in the spans)
+#pragma unroll
+        for (int q = 0; q < K; q++) bse[q] = base[q];
 
-        for (int st = 0; st < a.nsteps && !overflow; st++) {
-            const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)st;
+        for (int st = 0; st < inner && !overflow; st++) {
+            const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)(so + st);
             if (!PER) {
                 const uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
                 D.x0 = (int)bounded(sh.x, TX) + (d % ntx) * TX;
@@ -313,23 +466,70 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             if (st == 0) {
                 __syncthreads();  // the previous item's stores have read shared memory
                 if (tid == 0) *nslots = 0;
-                {
-                    // each thread owns one x column of the tile: rows r = y + TY z
-                    int gx = D.x0 + cx; gx -= gx >= L ? L : 0;
+                const bool few = nchains <= THREADS;  // few rings: find monomer 0 through the records
+                if (PER) {
+                    // each thread owns one x column of the box: rows r = y + TY z
                     for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
+                        const int y = r % TY, z = r / TY;
+                        cp_async4(S + cx + SX * y + SXY * z, lat + (uint32_t)(cx + L * (y + L * z)));
+                    }
+                    cp_async_wait_all();
+                    __syncthreads();
+                    if (!few) {
+                        for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
+                            const int idx = cx + SX * (r % TY) + SXY * (r / TY);
+                            const uint32_t wv = S[idx];
+                            if (wv & ELP_LBIT) S[idx] = take_slot<CAP>(wv, idx, rec, nslots, slot_chain, slot_off, slot_site);
+                        }
+                    }
+                } else {
+                    // rows r = y + TY z: the 16-byte aligned span [xa, xa + TX + 4)
+                    // of the box row in 16-byte granules (a granule never
+                    // straddles x = L: L and xa are multiples of 4)
+                    const int xa = D.x0 & ~3, sh = D.x0 & 3;
+                    D.ox = SH::OX + sh;
+#pragma unroll
+                    for (int q = 0; q < K; q++) bse[q] = base[q] + sh;
+                    constexpr int CPR = SH::SPAN / 4;
+                    for (int i = tid; i < SH::R * CPR; i += THREADS) {
+                        const int r = i / CPR, c = i - r * CPR;
                         const int y = r % TY, z = r / TY;
                         int gy = D.y0 + y; gy -= gy >= L ? L : 0;
                         int gz = D.z0 + z; gz -= gz >= L ? L : 0;
-                        cp_async4(S + SH::OX + cx + SX * y + SXY * z, lat + (uint32_t)(gx + L * (gy + L * gz)));
+                        int gx = xa + 4 * c; gx -= gx >= L ? L : 0;
+                        cp_async16(S + SH::OX + SX * y + SXY * z + 4 * c, lat + (uint32_t)(gx + L * (gy + L * gz)));
                     }
+                    cp_async_wait_all();
+                    __syncthreads();
+                    // span words outside the tile become halo words; with many
+                    // rings, monomer 0's runs are found in the same pass
+                    for (int i = tid; i < SH::R * CPR; i += THREADS) {
+                        const int r = i / CPR, c = i - r * CPR;
+                        const int at = SH::OX + SX * (r % TY) + SXY * (r / TY) + 4 * c;
+                        const int p0 = 4 * c - sh;  // tile column of the chunk's first word
+                        uint4 v = *reinterpret_cast<const uint4*>(S + at);
+                        const bool edge = p0 < 0 || p0 + 4 > TX;
+                        if (edge) {
+                            v.x = (unsigned)(p0 + 0) < (unsigned)TX ? v.x : HWALL;
+                            v.y = (unsigned)(p0 + 1) < (unsigned)TX ? v.y : HWALL;
+                            v.z = (unsigned)(p0 + 2) < (unsigned)TX ? v.z : HWALL;
+                            v.w = (unsigned)(p0 + 3) < (unsigned)TX ? v.w : HWALL;
+                        }
+                        if (!few && ((v.x | v.y | v.z | v.w) & ELP_LBIT)) {
+                            if (v.x & ELP_LBIT) v.x = take_slot<CAP>(v.x, at + 0, rec, nslots, slot_chain, slot_off, slot_site);
+                            if (v.y & ELP_LBIT) v.y = take_slot<CAP>(v.y, at + 1, rec, nslots, slot_chain, slot_off, slot_site);
+                            if (v.z & ELP_LBIT) v.z = take_slot<CAP>(v.z, at + 2, rec, nslots, slot_chain, slot_off, slot_site);
+                            if (v.w & ELP_LBIT) v.w = take_slot<CAP>(v.w, at + 3, rec, nslots, slot_chain, slot_off, slot_site);
+                            *reinterpret_cast<uint4*>(S + at) = v;
+                        } else if (edge) {
+                            *reinterpret_cast<uint4*>(S + at) = v;
+                        }
+                    }
+                    if (few) __syncthreads();
                 }
-                cp_async_wait_all();
-                __syncthreads();
-                // monomer-0 runs: global chain id -> shared slot, run length inline.
-                // Few rings: find them through the chain records; many: scan the tile.
-                if (nchains <= THREADS) {
+                if (few) {
                     for (int ch = tid; ch < nchains; ch += THREADS) {
-                        const uint4 r = *reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)ch);
+                        const uint4 r = __ldcg(reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)ch));
                         const int gx = (int)(r.x % (uint32_t)L), gy = (int)((r.x / (uint32_t)L) % (uint32_t)L),
                                   gz = (int)(r.x / ((uint32_t)L * L));
                         int x = gx - D.x0; x += x < 0 ? L : 0;
@@ -338,28 +538,11 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                         if (x < TX && y < TY && z < TZ) {
                             const uint32_t slot = atomicAdd(nslots, 1u);
                             if (slot < (uint32_t)CAP) {
-                                const int idx = SH::OX + x + SX * y + SXY * z;
+                                const int idx = D.ox + x + SX * y + SXY * z;
                                 slot_chain[slot] = (uint32_t)ch;
                                 slot_off[slot] = r.z;
                                 slot_site[slot] = idx;
                                 S[idx] = (S[idx] & 15) | ELP_LBIT | (slot << 5) | (r.y << ELP_CSHIFT);
-                            }
-                        }
-                    }
-                } else {
-                    for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
-                        const int y = r % TY, z = r / TY;
-                        const int idx = SH::OX + cx + SX * y + SXY * z;
-                        const uint32_t wv = S[idx];
-                        if (wv & ELP_LBIT) {
-                            const uint32_t slot = atomicAdd(nslots, 1u);
-                            const uint32_t chain = wv >> 5;
-                            if (slot < (uint32_t)CAP) {
-                                const uint4 rr = *reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)chain);
-                                slot_chain[slot] = chain;
-                                slot_off[slot] = rr.z;
-                                slot_site[slot] = idx;
-                                S[idx] = (wv & 15) | ELP_LBIT | (slot << 5) | (rr.y << ELP_CSHIFT);
                             }
                         }
                     }
@@ -396,13 +579,13 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 for (int kk = 0; kk < 4; kk++) {
                     if (active)
                         accepted += substepK<K, PER, NC, TABW, OFFW, HTABW, LIN>(
-                            slot_off, slot_site, base, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d,
+                            slot_off, slot_site, bse, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d,
                             k + kk, key);
                     __syncthreads();
                 }
             }
         }
-        if (!overflow) {
+        if (!overflow && !abort) {
             const uint32_t ns = *nslots;
             for (uint32_t sl = tid; sl < ns; sl += THREADS) {
                 const int idx = slot_site[sl];
@@ -413,12 +596,33 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 S[idx] = (wv & 15) | ELP_LBIT | (chain << 5);
             }
             __syncthreads();
-            int gx = D.x0 + cx; gx -= gx >= L ? L : 0;
-            for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
-                const int y = r % TY, z = r / TY;
-                int gy = D.y0 + y; gy -= gy >= L ? L : 0;
-                int gz = D.z0 + z; gz -= gz >= L ? L : 0;
-                lat[(uint32_t)(gx + L * (gy + L * gz))] = S[SH::OX + cx + SX * y + SXY * z];
+            if (PER) {
+                for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
+                    const int y = r % TY, z = r / TY;
+                    lat[(uint32_t)(cx + L * (y + L * z))] = S[cx + SX * y + SXY * z];
+                }
+            } else {
+                // 16-byte stores of the span's chunks inside the tile, single
+                // words at its ragged ends (a chunk never straddles x = L)
+                const int xa = D.x0 & ~3, sh = D.x0 & 3;
+                constexpr int CPR = SH::SPAN / 4;
+                for (int i = tid; i < SH::R * CPR; i += THREADS) {
+                    const int r = i / CPR, c = i - r * CPR;
+                    const int y = r % TY, z = r / TY;
+                    int gy = D.y0 + y; gy -= gy >= L ? L : 0;
+                    int gz = D.z0 + z; gz -= gz >= L ? L : 0;
+                    int gx = xa + 4 * c; gx -= gx >= L ? L : 0;
+                    uint32_t* g = lat + (uint32_t)(gx + L * (gy + L * gz));
+                    const uint32_t* cp = S + SH::OX + SX * y + SXY * z + 4 * c;
+                    const int p0 = 4 * c - sh;
+                    if (p0 >= 0 && p0 + 4 <= TX) {
+                        *reinterpret_cast<uint4*>(g) = *reinterpret_cast<const uint4*>(cp);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            if ((unsigned)(p0 + k) < (unsigned)TX) g[k] = cp[k];
+                    }
+                }
             }
         }
         if (J.acc) {
@@ -427,6 +631,8 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             if ((tid & 31) == 0 && v) atomicAdd(J.acc, v);
         }
     }
+    }
+    if (!PER && a.nsteps > 1) grid_exit(a.grid_bar);
 }
 
 }  // namespace elp
@@ -452,8 +658,28 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
     int grid = l->args.nitems;
     if (grid > l->nsm * MINB) grid = l->nsm * MINB;
     if (grid < 1) return cudaSuccess;
-    k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
-    return cudaGetLastError();
+    if (PER || l->args.nsteps <= 1) {
+        k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
+        return cudaGetLastError();
+    }
+    // tiled, several steps: a cooperative launch (every CTA resident, or an
+    // error) of at most as many CTAs as fit on the device at once
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, THREADS, SH::BYTES);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorNotSupported;
+    if (grid > l->nsm * per_sm) grid = l->nsm * per_sm;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SH::BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, l->args);
 }
 
 // Launch (or, with check_only, test) the specialised kernel for a shape.
@@ -462,7 +688,7 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
 {
     const elp_geometry& g = l->geom;
-    if (l->args.nsteps > 1 && !g.periodic) return cudaErrorNotSupported;
+    if (l->args.nsteps > 1 && !g.periodic && !l->args.grid_bar) return cudaErrorNotSupported;
 // shape: tile edges, whole box or tiled, colour modulus, shared-memory
 // strides, slot capacity, anchors per thread, threads, min blocks per SM
 #define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_)                                        \
@@ -470,10 +696,10 @@ extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
         l->sxy == SXY_)                                                                                        \
         return l->linear ? launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, true>(l, s)        \
                          : launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, false>(l, s);
-    SHAPE(32, 32, 32, 0, 16, 35, 1190, 2048, 2, 1024, 1)
-    SHAPE(32, 32, 16, 0, 16, 35, 1190, 1024, 1, 1024, 1)
-    SHAPE(16, 16, 16, 0, 16, 19, 342, 512, 1, 256, 4)
-    SHAPE(48, 24, 24, 0, 16, 51, 1326, 2048, 2, 864, 1)
+    SHAPE(32, 32, 32, 0, 16, 40, 1364, 2048, 2, 1024, 1)
+    SHAPE(32, 32, 16, 0, 16, 40, 1364, 1024, 1, 1024, 1)
+    SHAPE(16, 16, 16, 0, 16, 24, 444, 512, 1, 256, 4)
+    SHAPE(48, 24, 24, 0, 16, 56, 1456, 2048, 2, 864, 1)
     SHAPE(16, 16, 16, 1, 16, 16, 256, 2048, 1, 256, 1)
     SHAPE(32, 32, 32, 1, 16, 33, 1056, 2048, 2, 1024, 1)
     SHAPE(24, 24, 24, 1, 24, 24, 576, 2048, 1, 576, 1)

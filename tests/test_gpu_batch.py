@@ -16,6 +16,8 @@ MIX = [
     dict(L=64, N=500, seed=1005),
     dict(L=64, N=90, seed=1006, periodic=0, tile=(32, 32, 16)),
     dict(L=32, N=100, seed=1007, periodic=0, tile=(32, 16, 8)),   # generic kernel
+    dict(L=64, N=300, seed=1008, steps_per_launch=10),            # tiled, 10 steps per launch
+    dict(L=48, N=100, seed=1009, steps_per_launch=4),             # tiled, 4 steps per launch
 ]
 
 

@@ -77,6 +77,45 @@ def test_multi_step_launches_equal_single_steps():
     assert np.array_equal(wa, wb) and np.array_equal(ra, rb)
 
 
+@pytest.mark.parametrize("L,N,kw,spl,steps", [
+    (64, 200, dict(periodic=0, tile=(32, 32, 32)), 4, 9),
+    (48, 100, dict(periodic=0, tile=(48, 24, 24)), 3, 7),
+    (32, 100, dict(periodic=0, tile=(16, 16, 16)), 5, 10),
+])
+def test_tiled_multi_step_launches_match_replay(L, N, kw, spl, steps):
+    """Tiled melts run several steps per cooperative launch (grid barrier
+    between steps); every launch boundary still matches the replay."""
+    seed = 2000 + L + N
+    m = elp.Melt(L=L, N=N, seed=seed, steps_per_launch=spl, **kw)
+    m.init_melt()
+    r = replay_for(m, seed)
+    start, bonds = efpol_start(L, N, m.P)
+    assert r.load(start, bonds) == 0
+    done = 0
+    while done < steps:
+        k = min(spl, steps - done)
+        m.run(k)
+        r.steps(k)
+        done += k
+        w, rec = m.state()
+        assert np.array_equal(w, r.lattice()), f"site words differ after step {done}"
+        assert np.array_equal(rec, r.records()), f"records differ after step {done}"
+    assert m.check() == 0
+    assert m.accepted() == r.accepted
+
+
+def test_tiled_steps_per_launch_do_not_change_bits():
+    states = []
+    for spl in (1, 3, 10, 64):
+        m = elp.Melt(L=64, N=200, seed=5, steps_per_launch=spl)
+        m.init_melt()
+        m.run(67)                  # graph replays (50, 48, 50 or 64 steps) plus single launches
+        states.append(m.state())
+        assert m.check() == 0
+    for w, rec in states[1:]:
+        assert np.array_equal(w, states[0][0]) and np.array_equal(rec, states[0][1])
+
+
 def test_initial_melt_is_reference_t0(tmp_path):
     m = elp.Melt(L=32, N=100, seed=1)
     m.init_melt()
