@@ -118,6 +118,9 @@ elp_status elp_device_errors(const uint32_t* d_flags, cudaStream_t s)
     if (flags & 1u)
         return elp_fail(ELP_ERR_STATE, "a domain held more monomer-0 runs than its label table; steps after the "
                                        "overflow are incomplete (use the generic kernel for this melt)");
+    if (flags & 4u)
+        return elp_fail(ELP_ERR_STATE, "a tiled launch of several steps gave up waiting at its grid barrier; steps "
+                                       "after it are incomplete");
     return ELP_OK;
 }
 

@@ -86,7 +86,7 @@ cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int 
     G->generic = generic;
     G->spl = spl > 0 ? spl : 1;
     G->use_graph = !geom.periodic;
-    G->graph_steps = 50;
+    G->graph_steps = 100;
     G->stream = stream;
     G->d_table = d_table;
     G->d_error = d_error;

@@ -23,7 +23,7 @@ struct elp_group {
     size_t smem;                      // its dynamic shared memory per block
     int spl;                          // steps per launch (tiled: specialised kernel only)
     int use_graph;                    // tiled domains: replay launches from a CUDA graph
-    int graph_steps;                  // launches captured per graph
+    int graph_steps;                  // steps captured per graph (rounded down to whole launches)
     cudaStream_t stream;
     const uint32_t* d_table;
     uint32_t* d_error;

@@ -8,7 +8,8 @@ struct SweepArgs {
     uint32_t* rec;                 // chain records
     const uint32_t* table;         // 1024 words = 4096 bytes dst1|dst2<<4
     unsigned long long* accepted;  // optional accepted-move counter
-    uint32_t* error;               // device error flags (bit 0: label slot table overflow)
+    uint32_t* error;               // device error flags (bit 0: label slot table overflow,
+                                   // bit 2: grid barrier wait gave up)
     int nchains;                   // rings in the melt
     int L, periodic, tx, ty, tz, ncol;
     int sx, sxy, ox, words, groups;

@@ -11,16 +11,16 @@
 //     (bits 5-15) into a small shared-memory table {chain, offset, site};
 //     the chain records in global memory are read when the tile is loaded and
 //     written back when it is stored, so no move waits on global memory;
-//   * a tile's rows are fetched by bulk copies (the TMA engine, one or two
-//     per row) that complete on a shared-memory mbarrier.  The origin shift
-//     makes a row start anywhere, so each copy takes the 16-byte aligned
-//     span around the row (TX + 4 words) and the tile sits sh = x0 mod 4
-//     words into it; the words of the span outside the tile become halo
-//     words.  Tiles go back with 16-byte stores (single words at the ragged
-//     ends).  Rows are 16-byte aligned in shared memory, and the threads of
-//     a warp take anchors from an 8 x 4 block of rows so that their first
-//     loads hit 32 different banks;
-//   * the grid is persistent over the tiles.
+//   * a tile's rows are fetched in 16-byte cp.async granules.  The origin
+//     shift makes a row start anywhere, so each row fetch takes the 16-byte
+//     aligned span around the row (TX + 4 words) and the tile sits
+//     sh = x0 mod 4 words into it; the words of the span outside the tile
+//     become halo words.  Tiles go back with 16-byte stores (single words at
+//     the ragged ends).  Rows are 16-byte aligned in shared memory, and the
+//     threads of a warp take anchors from an 8 x 4 block of rows so that
+//     their first loads hit 32 different banks;
+//   * the grid is persistent over the tiles, and a launch of several steps
+//     over a tiled box is cooperative, with a grid barrier between steps.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -41,66 +41,22 @@ __device__ __forceinline__ void cp_async16(uint32_t* sdst, const uint32_t* gsrc)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// ---- bulk copies (TMA engine, untiled) completing on a shared-memory mbarrier
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-// one arrival that also announces `bytes` of copies for the current phase
-__device__ __forceinline__ void mbar_arrive_expect(uint64_t* m, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* m, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(m)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Wait for phase `parity` of the mbarrier to complete, giving up after
-// `limit` polls (each poll may itself suspend the thread for a while).
-__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, int limit)
-{
-    for (int i = 0; i < limit; i++)
-        if (mbar_test(m, parity)) return true;
-    return false;
-}
-// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
-__device__ __forceinline__ void bulk_g2s(uint32_t* dst, const uint32_t* src, uint32_t bytes, uint64_t* m)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(m))
-                 : "memory");
-}
-// order this thread's earlier shared-memory accesses before later bulk copies
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-constexpr int MBAR_POLLS = 1 << 22;
-
 __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p)
 {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-// order generic-proxy accesses to global memory with bulk copies
-__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
 constexpr int GRID_POLLS = 1 << 24;
 
 // Barrier over all CTAs of a cooperative launch: each CTA adds one to
 // bar[0] and waits (bounded) until it reaches `target`.  The CTA's stores
-// before it are visible to every CTA's loads and bulk copies after it.
+// before it are visible to every CTA's loads after it (tiles are fetched
+// with cp.async.cg and records with ld.global.cg, both through L2).
 // Returns false, in every thread of the CTA, when the wait gave up.
 __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t target)
 {
     bool ok = true;
-    fence_proxy_async_global();
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -110,9 +66,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t target)
             __nanosleep(64);
         }
     }
-    const bool failed = __syncthreads_or(!ok) != 0;
-    fence_proxy_async_global();
-    return !failed;
+    return __syncthreads_or(!ok) == 0;
 }
 // Last act of every CTA of a cooperative launch: the last one to leave
 // zeroes the barrier counts for the next launch on the stream.
@@ -143,8 +97,8 @@ struct Shape {
     static constexpr bool PERM = !PER && TY % 8 == 0 && TZ % 4 == 0 && AT % R == 0;
     // shared-memory word offsets: lattice, transition table (4096 bytes),
     // neighbour offsets (27 x 16), colours, slot tables, slot count, the
-    // Philox words of the current substep group when threads own < 4 anchors,
-    // and the mbarrier of the tile copies
+    // and the Philox words of the current and the next substep group when
+    // threads own < 4 anchors
     static constexpr int TABW = WORDS;
     static constexpr int OFFW = TABW + 1024;
     static constexpr int COLW = OFFW + 27 * 16;
@@ -154,8 +108,8 @@ struct Shape {
     static constexpr int NSLW = SSIW + CAP;
     static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
     static constexpr int RNDW = (HTABW + 64 + 4) & ~3;
-    static constexpr int MBW = RNDW + (K < 4 ? 4 * G : 0);
-    static constexpr int TOTW = MBW + 4;
+    // two buffers of Philox words: the next group's are drawn during this one
+    static constexpr int TOTW = RNDW + (K < 4 ? 8 * G : 0);
     static constexpr size_t BYTES = (size_t)TOTW * 4;
     static_assert(PER || (SX % 4 == 0 && SXY % 4 == 0 && SX >= SPAN + 1 && SXY >= SX * (TY + 2)),
                   "tiled rows: 16-byte aligned, room for the span and the halo word before it");
@@ -190,34 +144,37 @@ __device__ __forceinline__ uint32_t take_slot(uint32_t wv, int idx, const uint32
     return (wv & 15) | ELP_LBIT | (slot << 5) | (rr.y << ELP_CSHIFT);
 }
 
+// Shared-memory word at byte offset b (offsets are kept in bytes so that a
+// load or store needs no index scaling).
+__device__ __forceinline__ uint32_t& SW(int b) { return *reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(g_smem) + b); }
+
 // The K anchors of one thread, one substep.  Returns accepted moves.
 // Anchor q takes its random byte at bit offset bsh[q] of the Philox word w.
-// Shared-memory word indices: lattice at 0, transition table (bytes) at
-// TABW words, neighbour offsets at OFFW words.
+// Byte offsets: anchors base4 + 4 xr, colour c4 = 4 c, neighbour offsets at
+// OFFW words; transition table (bytes) at TABW words.
 template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW, bool LIN>
-__device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, const int (&base)[K], const int (&rot)[K],
-                                        const int (&clsyz)[K], const int (&xj)[K], const int (&bsh)[K],
-                                        const int (&an)[K], int c, uint32_t w, int L, bool lin, uint32_t t, int d,
+__device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, const int (&base4)[K], const int (&rot4)[K],
+                                        const int (&clsyz)[K], const int (&xj4)[K], const int (&bsh)[K],
+                                        const int (&an)[K], int c4, uint32_t w, int L, bool lin, uint32_t t, int d,
                                         int k, uint2 key)
 {
-    uint32_t* S = g_smem;
     const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
     const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
     int p[K], ob[K];
     uint32_t wP[K], rb[K];
 #pragma unroll
     for (int q = 0; q < K; q++) {
-        int xr = c + rot[q];
-        if ((NC & (NC - 1)) == 0) xr &= NC - 1;
-        else xr -= xr >= NC ? NC : 0;
-        p[q] = base[q] + xr;
+        int xr4 = c4 + rot4[q];
+        if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
+        else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
+        p[q] = base4[q] + xr4;
         int cls = clsyz[q];
         if (PER) {
-            int x = xr + xj[q];
-            cls += x == 0 ? 0 : (x == L - 1 ? 2 : 1);
+            int x4 = xr4 + xj4[q];
+            cls += x4 == 0 ? 0 : (x4 == 4 * (L - 1) ? 2 : 1);
         }
         ob[q] = 16 * cls;
-        wP[q] = S[p[q]];
+        wP[q] = SW(p[q]);
         rb[q] = (w >> bsh[q]) & 0xffu;
     }
     // stage B: the next run (slot 1).  Loaded unconditionally: the index is
@@ -228,7 +185,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
 #pragma unroll
     for (int q = 0; q < K; q++) {
         pB[q] = p[q] + offs[ob[q] + (wP[q] & 15)];
-        wB[q] = S[pB[q]];
+        wB[q] = SW(pB[q]);
     }
     // stage C: source bonds (b_{m-1}, b_m) and the table option.  Slot 0
     // (last monomer of P's run) uses row (0, b_out(P)) when the run holds two
@@ -250,7 +207,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
 #pragma unroll
     for (int q = 0; q < K; q++) {
         pY[q] = p[q] + offs[ob[q] + (e[q] & 15)];
-        wY[q] = S[pY[q]];
+        wY[q] = SW(pY[q]);
     }
     // stage E: accept, label bookkeeping, write.  Store order B, Y, P: when
     // dst1 == 0 the target is P itself and P's store must come last.
@@ -287,11 +244,11 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
             if (src == 0) nP &= ~LMASK; else if (src == 1) nB &= ~LMASK; else nY &= ~LMASK;
             if (nl == 0) nP |= lb; else if (nl == 1) nB |= lb; else nY |= lb;
             slot_off[slot] = noff;
-            slot_site[slot] = nl == 0 ? p[q] : (nl == 1 ? pB[q] : pY[q]);
+            slot_site[slot] = (nl == 0 ? p[q] : (nl == 1 ? pB[q] : pY[q])) >> 2;
         }
-        if (ok && s) S[pB[q]] = nB;
-        if (ok && d1) S[pY[q]] = nY;
-        if (ok) S[p[q]] = nP;
+        if (ok && s) SW(pB[q]) = nB;
+        if (ok && d1) SW(pY[q]) = nY;
+        if (ok) SW(p[q]) = nP;
         if (LIN) wP[q] = ok ? nP : wP[q];
         acc += ok ? 1 : 0;
     }
@@ -314,19 +271,19 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
             const uint32_t d2 = e >> 4, slot = (w0 >> 5) & 0x7FFu;
             if (cP >= 2) {
                 const int pY = p[q] + offs[ob[q] + ((~d2) & 15u)];
-                if (S[pY] == 0) {
-                    S[pY] = d2 | (w0 & LMASK) | ELP_CUNIT;
-                    S[p[q]] = (w0 & ~LMASK) - ELP_CUNIT;
-                    slot_site[slot] = pY;
+                if (SW(pY) == 0) {
+                    SW(pY) = d2 | (w0 & LMASK) | ELP_CUNIT;
+                    SW(p[q]) = (w0 & ~LMASK) - ELP_CUNIT;
+                    slot_site[slot] = pY >> 2;
                     acc++;
                 }
             } else {
                 const int pB = p[q] + offs[ob[q] + bo];
-                const uint32_t wB = S[pB];
+                const uint32_t wB = SW(pB);
                 if (wB != HWALL) {
-                    S[pB] = (wB + ELP_CUNIT) | (w0 & LMASK);
-                    S[p[q]] = 0;
-                    slot_site[slot] = pB;
+                    SW(pB) = (wB + ELP_CUNIT) | (w0 & LMASK);
+                    SW(p[q]) = 0;
+                    slot_site[slot] = pB >> 2;
                     acc++;
                 }
             }
@@ -385,14 +342,10 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             if (cz == 0 && dv < 0) dv = LP - 1;
             if (cz == 2 && dv > 0) dv = -(LP - 1);
         }
-        offs[i] = dt + SX * du + SXY * dv;
+        offs[i] = 4 * (dt + SX * du + SXY * dv);   // bytes
     }
     if (!PER)
         for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = HWALL;
-
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(g_smem + SH::MBW);
-    if (!PER && tid == 0) mbar_init(mbar, 1);
-    uint32_t mbar_phase = 0;
 
     // Anchor an = g + q G of a substep takes byte q of Philox word g.  Thread
     // tid owns anchors an = tid + q AT, or with PERM the anchors of the same
@@ -413,12 +366,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         int j = an / SH::R, row = an % SH::R;
         int y = row % TY, z = row / TY;
         int m = (2 * y + 3 * z) % NC;
-        rot[q] = m ? NC - m : 0;
-        base[q] = SH::OX + SX * y + SXY * z + NC * j;
+        rot[q] = 4 * (m ? NC - m : 0);                       // bytes
+        base[q] = 4 * (SH::OX + SX * y + SXY * z + NC * j);  // bytes
         int cy = y == 0 ? 0 : (y == LP - 1 ? 2 : 1);
         int cz = z == 0 ? 0 : (z == LP - 1 ? 2 : 1);
         clsyz[q] = PER ? (3 * cy + 9 * cz) : 13;
-        xj[q] = NC * j;
+        xj[q] = 4 * NC * j;
     }
     const bool active = tid < SH::AT;
     const uint32_t step_dev = a.step_dev ? *a.step_dev : 0u;
@@ -427,14 +380,13 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     // steps one after another over all tiles, with a grid barrier between
     // steps (the launch is cooperative: all CTAs are resident).
     const int outer = PER ? 1 : a.nsteps, inner = PER ? a.nsteps : 1;
-    bool abort = false;
 
-    for (int so = 0; so < outer && !abort; so++) {
+    for (int so = 0; so < outer; so++) {
     if (so > 0 && !grid_barrier(a.grid_bar, gridDim.x * (uint32_t)so)) {
         if (tid == 0) atomicOr(a.error, 4u);
         break;
     }
-    for (int it = blockIdx.x; it < a.nitems && !abort; it += gridDim.x) {
+    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
         const uint2 item = a.items[it];
         const BatchJob& J = a.jobs[item.x];
         const int d = (int)item.y;
@@ -451,7 +403,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         D.x0 = 0; D.y0 = 0; D.z0 = 0;
         int accepted = 0;
         bool overflow = false;
-        int bse[K];   // anchor base indices of this tile (plus its offset sh in the spans)
+        int bse[K];   // anchor base byte offsets of this tile (plus its offset sh in the spans)
 #pragma unroll
         for (int q = 0; q < K; q++) bse[q] = base[q];
 
@@ -489,7 +441,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                     const int xa = D.x0 & ~3, sh = D.x0 & 3;
                     D.ox = SH::OX + sh;
 #pragma unroll
-                    for (int q = 0; q < K; q++) bse[q] = base[q] + sh;
+                    for (int q = 0; q < K; q++) bse[q] = base[q] + 4 * sh;
                     constexpr int CPR = SH::SPAN / 4;
                     for (int i = tid; i < SH::R * CPR; i += THREADS) {
                         const int r = i / CPR, c = i - r * CPR;
@@ -548,12 +500,13 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                     }
                 }
             }
+            if (K < 4 && tid < SH::G) rnd[tid] = philox(make_uint4(t, (uint32_t)d, 0u, (uint32_t)tid), key);
             if (tid < (2 * NC + 3) / 4) {
                 const uint4 cw = philox(make_uint4(t, (uint32_t)d, (uint32_t)tid | ELP_STREAM_COLOUR, 0), key);
-                col[4 * tid + 0] = bounded(cw.x, NC);
-                col[4 * tid + 1] = bounded(cw.y, NC);
-                col[4 * tid + 2] = bounded(cw.z, NC);
-                col[4 * tid + 3] = bounded(cw.w, NC);
+                col[4 * tid + 0] = 4 * bounded(cw.x, NC);   // colours in bytes of x offset
+                col[4 * tid + 1] = 4 * bounded(cw.y, NC);
+                col[4 * tid + 2] = 4 * bounded(cw.z, NC);
+                col[4 * tid + 3] = 4 * bounded(cw.w, NC);
             }
             __syncthreads();
             if (*nslots > (uint32_t)CAP) {
@@ -568,11 +521,14 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 if (K == 4) {
                     if (active) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
                 } else {
-                    // G threads draw the group's words; the other reads of rnd
-                    // (previous group) are four barriers behind
-                    if (tid < SH::G) rnd[tid] = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
-                    __syncthreads();
-                    if (active) rw = rnd[gq];
+                    // this group's words were drawn during the previous one (or
+                    // before the first); G threads now draw the next group's
+                    // into the other buffer, read four barriers ago
+                    const int cur = (k >> 2) & 1;
+                    if (active) rw = rnd[cur * SH::G + gq];
+                    if (tid < SH::G && k + 4 < 2 * NC)
+                        rnd[(cur ^ 1) * SH::G + tid] =
+                            philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2) + 1u, (uint32_t)tid), key);
                 }
                 const uint32_t rws[4] = {rw.x, rw.y, rw.z, rw.w};
 #pragma unroll
@@ -585,7 +541,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 }
             }
         }
-        if (!overflow && !abort) {
+        if (!overflow) {
             const uint32_t ns = *nslots;
             for (uint32_t sl = tid; sl < ns; sl += THREADS) {
                 const int idx = slot_site[sl];
@@ -664,10 +620,14 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
     }
     // tiled, several steps: a cooperative launch (every CTA resident, or an
     // error) of at most as many CTAs as fit on the device at once
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, THREADS, SH::BYTES);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorNotSupported;
+    static int per_sm = 0;   // resident CTAs per SM of this kernel (same on every device of the pool)
+    if (per_sm < 1) {
+        int n = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, THREADS, SH::BYTES);
+        if (e != cudaSuccess) return e;
+        if (n < 1) return cudaErrorNotSupported;
+        per_sm = n;
+    }
     if (grid > l->nsm * per_sm) grid = l->nsm * per_sm;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
@@ -696,7 +656,7 @@ extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
         l->sxy == SXY_)                                                                                        \
         return l->linear ? launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, true>(l, s)        \
                          : launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, false>(l, s);
-    SHAPE(32, 32, 32, 0, 16, 40, 1364, 2048, 2, 1024, 1)
+    SHAPE(32, 32, 32, 0, 16, 40, 1364, 1792, 2, 1024, 1)
     SHAPE(32, 32, 16, 0, 16, 40, 1364, 1024, 1, 1024, 1)
     SHAPE(16, 16, 16, 0, 16, 24, 444, 512, 1, 256, 4)
     SHAPE(48, 24, 24, 0, 16, 56, 1456, 2048, 2, 864, 1)

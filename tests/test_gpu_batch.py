@@ -24,29 +24,29 @@ MIX = [
 def test_batch_members_equal_single_runs():
     b = elp.Batch(MIX)
     b.init_melts()
-    b.run(60)                      # tiled groups: one 50-launch graph + 10 launches
+    b.run(130)                     # tiled groups: one 100-step graph + 30 launches
     b.sync()
     for j, kw in enumerate(MIX):
         m = elp.Melt(**kw)
         m.init_melt()
-        m.run(60)
+        m.run(130)
         wa, ra = b.state(j)
         wb, rb = m.state()
         assert np.array_equal(wa, wb) and np.array_equal(ra, rb), f"melt {j} differs from its single run"
         assert b.accepted(j) == m.accepted()
         assert b.check(j) == 0
-        assert b.info(j).step == 60
+        assert b.info(j).step == 130
 
 
 def test_batch_graph_replays_continue_the_stream():
     kw = dict(L=64, N=500, seed=77)
     b = elp.Batch([kw, dict(L=16, N=50, seed=78)])
     b.init_melts()
-    for n in (50, 50, 7, 100):     # graph, replay, single launches, two replays
+    for n in (100, 100, 7, 200):   # graph, replay, single launches, two replays
         b.run(n)
     m = elp.Melt(**kw)
     m.init_melt()
-    m.run(207)
+    m.run(407)
     wa, ra = b.state(0)
     wb, rb = m.state()
     assert np.array_equal(wa, wb) and np.array_equal(ra, rb)

@@ -109,7 +109,7 @@ def test_tiled_steps_per_launch_do_not_change_bits():
     for spl in (1, 3, 10, 64):
         m = elp.Melt(L=64, N=200, seed=5, steps_per_launch=spl)
         m.init_melt()
-        m.run(67)                  # graph replays (50, 48, 50 or 64 steps) plus single launches
+        m.run(167)                 # graph replays (100, 99, 100 or 2 x 64 steps) plus single launches
         states.append(m.state())
         assert m.check() == 0
     for w, rec in states[1:]:
