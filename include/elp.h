@@ -202,6 +202,13 @@ elp_status elp_scaleup_tuv(const char* in_path, const char* out_path);
  * pol_id is out of range. */
 elp_status elp_tuv_to_xyz(const char* in_path, int32_t pol_id, const char* out_path);
 
+/* The chains of a TUV file as a POV-Ray scene (analysis/tuv2pov.c): camera
+ * and area light placed as the reference places them, a cylinder per link
+ * and a sphere per site, coloured by chain (pol_id < 0: all chains) or along
+ * the one chain pol_id.  The scene text is the reference's byte for byte.
+ * Host only; ELP_ERR_ARG if pol_id >= np. */
+elp_status elp_tuv_to_pov(const char* in_path, const char* out_path, int32_t pol_id);
+
 /* ---- PTL writer --------------------------------------------------------------
  * Per-ring time series written while a run dumps: sample_dir/ptl/pol=<p>_dev=<dev>.res,
  * the files the reference's create_ptl makes afterwards from the run's TUV

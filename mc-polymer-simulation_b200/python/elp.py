@@ -49,6 +49,7 @@ EXPORTED = [
     "elp_server_default_opts", "elp_server_create", "elp_server_submit", "elp_server_poll", "elp_server_get_stats",
     "elp_server_drain", "elp_server_destroy", "elp_check_noalloc", "elp_observe", "elp_batch_observe",
     "elp_ptl_open", "elp_ptl_append", "elp_ptl_close", "elp_double_chains",
+    "elp_scaleup_tuv", "elp_tuv_to_xyz", "elp_tuv_to_pov",
 ]
 
 OBS_MAX_BINS = 64
@@ -114,6 +115,9 @@ def lib():
         "elp_ptl_append": (i32, [vp, vp, vp]),
         "elp_ptl_close": (i32, [vp]),
         "elp_double_chains": (i32, [i32, i32, i32, vp, vp, vp, vp]),
+        "elp_scaleup_tuv": (i32, [C.c_char_p, C.c_char_p]),
+        "elp_tuv_to_xyz": (i32, [C.c_char_p, i32, C.c_char_p]),
+        "elp_tuv_to_pov": (i32, [C.c_char_p, C.c_char_p, i32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -25,7 +25,9 @@ It compiles the reference's efpol from its own sources (oracle/Makefile target
 * ``scaleup_<input>.res.gz`` -- the reference's analysis/scaleup.c output
   for three of the TUV files above (compact t=0 rings and relaxed melts);
   ``xyz_efpol_L16_N50_s3_t100_p{0,3,97}.txt.gz`` -- its analysis/tuv2xyz.c
-  export of three rings;
+  export of three rings; ``pov_efpol_L16_N50_s3_t100_p3.pov.gz`` -- its
+  analysis/tuv2pov.c scene of one ring, and ``pov_sha256.json`` the SHA-256
+  of its whole-melt scenes (rings and linear chains);
 * ``efpol_lin_*`` -- the same for linear chains (the reference built with
   POL_TYPE=POL_LIN as efpol_lin): ``efpol_lin_L32_N100_s1_t{0,100,200}``,
   ``efpol_lin_L16_N50_s3_t{0..100}`` and ``efpol_lin_stats_L16_N50.json`` /
@@ -41,6 +43,7 @@ from __future__ import annotations
 
 import argparse
 import gzip
+import hashlib
 import json
 import os
 import shutil
@@ -127,6 +130,29 @@ def make_export(refdir, tmp):
             g.write(f.read())
 
 
+def make_pov(refdir, tmp):
+    """The reference's tuv2pov on committed reference TUV files: one chain's
+    scene in full, and the SHA-256 of whole-melt scenes (megabytes of text)."""
+    hashes = {}
+    for name, pids in (("efpol_L16_N50_s3_t100", (3, -1)), ("efpol_lin_L32_N100_s1_t200", (0, -1)),
+                       ("efpol_L32_N100_s1_t0", (-1,))):
+        src = os.path.join(tmp, name + ".res")
+        with gzip.open(os.path.join(HERE, name + ".res.gz"), "rb") as f, open(src, "wb") as g:
+            g.write(f.read())
+        for pid in pids:
+            dst = os.path.join(tmp, f"pov_{name}_{pid}.pov")
+            args = [os.path.join(refdir, "tuv2pov"), src, dst] + ([str(pid)] if pid >= 0 else [])
+            subprocess.run(args, check=True, stdout=subprocess.DEVNULL)
+            with open(dst, "rb") as f:
+                data = f.read()
+            hashes[f"{name}/{pid}"] = hashlib.sha256(data).hexdigest()
+            if pid >= 0 and name.startswith("efpol_L16"):
+                with gzip.GzipFile(os.path.join(HERE, f"pov_{name}_p{pid}.pov.gz"), "wb", mtime=0) as g:
+                    g.write(data)
+    with open(os.path.join(HERE, "pov_sha256.json"), "w") as f:
+        json.dump(hashes, f, indent=1, sort_keys=True)
+
+
 def make_linear(refdir, tmp):
     """efpol_lin: initial melt, short trajectories and ensemble statistics."""
     lin = os.path.join(refdir, "efpol_lin")
@@ -165,7 +191,7 @@ def write_stats(binary, prefix, engine, cases, tmp):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["all", "ptl", "double", "export", "linear"], default="all")
+    ap.add_argument("--only", choices=["all", "ptl", "double", "export", "pov", "linear"], default="all")
     args = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={args.ref}"], check=True,
                    stdout=subprocess.DEVNULL)
@@ -181,6 +207,9 @@ def main():
             return
         if args.only == "export":
             make_export(refdir, tmp)
+            return
+        if args.only == "pov":
+            make_pov(refdir, tmp)
             return
         if args.only == "linear":
             make_linear(refdir, tmp)
@@ -206,6 +235,7 @@ def main():
         make_ptl(refdir, efpol, tmp)
         make_double(efpol, tmp)
         make_export(refdir, tmp)
+        make_pov(refdir, tmp)
         make_linear(refdir, tmp)
 
         # efpol's seeding drops bit 0 of every Tausworthe word (util/rng.h:13-20,

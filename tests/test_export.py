@@ -1,11 +1,15 @@
 """Host tools around the melt files against the reference's own tools.
 
-tests/golden/scaleup_*.res.gz and xyz_*.txt.gz were written by the
-reference's analysis/scaleup.c and analysis/tuv2xyz.c (built from its
-sources, tests/golden/make_golden.py) from committed reference TUV files.
-elp_scaleup_tuv / elp_tuv_to_xyz, and the drop-in programs bin/scaleup and
-bin/tuv2xyz built on them, must write the same bytes and exit codes."""
+tests/golden/scaleup_*.res.gz, xyz_*.txt.gz, pov_*.pov.gz and
+pov_sha256.json were written by the reference's analysis/scaleup.c,
+analysis/tuv2xyz.c and analysis/tuv2pov.c (built from its sources,
+tests/golden/make_golden.py) from committed reference TUV files.
+elp_scaleup_tuv / elp_tuv_to_xyz / elp_tuv_to_pov, and the drop-in programs
+bin/scaleup, bin/tuv2xyz and bin/tuv2pov built on them, must write the same
+bytes and exit codes."""
 import gzip
+import hashlib
+import json
 import os
 import subprocess
 
@@ -60,3 +64,36 @@ def test_tools_exit_codes(tmp_path):
                           capture_output=True).returncode == 192
     assert subprocess.run([os.path.join(BIN, "tuv2xyz"), str(src), str(tmp_path / "o"), "98"],
                           capture_output=True).returncode == 193
+
+
+def test_tuv2pov_one_ring_matches_reference(tmp_path):
+    src = unpack(tmp_path, "efpol_L16_N50_s3_t100.res.gz")
+    want = gzip.open(os.path.join(GOLD, "pov_efpol_L16_N50_s3_t100_p3.pov.gz"), "rb").read()
+    out = tmp_path / "lib.pov"
+    elp.check(elp.lib().elp_tuv_to_pov(str(src).encode(), str(out).encode(), 3))
+    assert out.read_bytes() == want
+    cli = tmp_path / "cli.pov"
+    assert subprocess.run([os.path.join(BIN, "tuv2pov"), str(src), str(cli), "3"], timeout=60).returncode == 0
+    assert cli.read_bytes() == want
+
+
+@pytest.mark.parametrize("key", ["efpol_L16_N50_s3_t100/-1", "efpol_L32_N100_s1_t0/-1",
+                                 "efpol_lin_L32_N100_s1_t200/-1", "efpol_lin_L32_N100_s1_t200/0"])
+def test_tuv2pov_scenes_match_reference(tmp_path, key):
+    """Whole-melt scenes (rings, compact t=0 rings, linear chains) and one
+    linear chain: the SHA-256 of the reference's scene text."""
+    name, pid = key.split("/")
+    want = json.load(open(os.path.join(GOLD, "pov_sha256.json")))[key]
+    src = unpack(tmp_path, name + ".res.gz")
+    out = tmp_path / "s.pov"
+    args = [os.path.join(BIN, "tuv2pov"), str(src), str(out)] + ([pid] if int(pid) >= 0 else [])
+    assert subprocess.run(args, timeout=60).returncode == 0
+    assert hashlib.sha256(out.read_bytes()).hexdigest() == want
+
+
+def test_tuv2pov_exit_codes(tmp_path):
+    src = unpack(tmp_path, "efpol_L16_N50_s3_t100.res.gz")
+    run = lambda *a: subprocess.run([os.path.join(BIN, "tuv2pov")] + [str(x) for x in a], capture_output=True)
+    assert run(src).returncode == 192                                   # missing POV_FILE
+    assert run(tmp_path / "missing.res", tmp_path / "o.pov").returncode == 192
+    assert run(src, tmp_path / "o.pov", 98).returncode == 193           # np= 98: chains 0..97
