@@ -316,7 +316,9 @@ typedef struct elp_server_stats {
 void elp_server_default_opts(elp_server_opts* o);
 elp_status elp_server_create(const elp_server_opts* opts, elp_server** out);
 /* Queue a job: initial melt of `spec`, `nsteps` steps, a TUV dump every
- * `dump_interval` steps (0: none) and at the end.  Thread-safe. */
+ * `dump_interval` steps (0: none) and at the end.  Thread-safe.  Ring and
+ * linear-chain jobs run in separate groups; a linear-chain job whose box has
+ * no specialised kernel shape finishes with status ELP_ERR_ARG. */
 elp_status elp_server_submit(elp_server* s, const elp_job_spec* spec, int64_t nsteps, int64_t dump_interval,
                              const char* dump_dir, uint64_t* id);
 /* Move up to `cap` finished jobs' results to `out`; *n receives the count. */

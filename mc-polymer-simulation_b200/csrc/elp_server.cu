@@ -81,7 +81,7 @@ struct Snap {
 };
 
 struct SGroup {
-    std::tuple<int, int, int, int, int, int> key;
+    std::tuple<int, int, int, int, int, int, int> key;   // geometry, linear chains
     elp_group G;
     cudaStream_t s = nullptr;
     cudaEvent_t ev = nullptr;             // end of the running tick
@@ -156,10 +156,11 @@ static void io_worker(elp_server* s)
         start.resize((size_t)P * 3);
         bonds.resize((size_t)P * N);
         cudaStreamWaitEvent(st, sn.ready, 0);
-        elp_status rc = elp_fetch_rings(sn.d_lat, sn.d_rec, L, N, P, 0, &wb, start.data(), bonds.data(), st);
+        const int lin = j->spec.linear ? 1 : 0;
+        elp_status rc = elp_fetch_rings(sn.d_lat, sn.d_rec, L, N, P, lin, &wb, start.data(), bonds.data(), st);
         if (sn.final && rc == ELP_OK) {
             int32_t code = -1;
-            if (elp_check_melt(sn.d_lat, sn.d_rec, L, N, P, 0, &wb, &code, st) == ELP_OK) j->integrity = code;
+            if (elp_check_melt(sn.d_lat, sn.d_rec, L, N, P, lin, &wb, &code, st) == ELP_OK) j->integrity = code;
         }
         std::string err = rc == ELP_OK ? std::string() : std::string(elp_last_error());
         cudaFreeAsync(sn.d_lat, st);
@@ -203,7 +204,7 @@ static void io_worker(elp_server* s)
 
 static SGroup* group_for(elp_server* s, SJob* j)
 {
-    auto key = std::make_tuple(j->g.periodic, j->g.L, j->g.tx, j->g.ty, j->g.tz, j->g.ncol);
+    auto key = std::make_tuple(j->g.periodic, j->g.L, j->g.tx, j->g.ty, j->g.tz, j->g.ncol, j->spec.linear ? 1 : 0);
     for (auto& gp : s->groups)
         if (gp->key == key) return gp.get();
     if (s->groups.size() >= 64) return nullptr;
@@ -266,7 +267,7 @@ static bool admit(elp_server* s)
         }
         // the initial melt is written on the device, ordered on the group's
         // stream behind its running steps: the scheduler does not wait
-        if (elp_init_melt_device(j->lat, j->rec, j->g.L, j->spec.N, j->P, 0, gp->s) != ELP_OK) {
+        if (elp_init_melt_device(j->lat, j->rec, j->g.L, j->spec.N, j->P, j->spec.linear ? 1 : 0, gp->s) != ELP_OK) {
             cudaFreeAsync(j->lat, gp->s);
             cudaFreeAsync(j->rec, gp->s);
             fail_job(s, j, ELP_ERR_ARG, "initial melt does not fit the box");
@@ -296,11 +297,28 @@ static bool rebuild(elp_server* s, SGroup* gp)
         SJob* j = gp->members[i];
         j->index = (int)i;
         elp_group_add(&G, j->lat, j->rec, s->d_acc, j->spec.N, j->P, j->spec.seed, j->spec.salt,
-                      (uint64_t)j->done_steps, 0);
+                      (uint64_t)j->done_steps, j->spec.linear ? 1 : 0);
     }
     gp->dirty = false;
     if (gp->members.empty()) return true;
-    return elp_group_commit(&G) == cudaSuccess;
+    if (elp_group_commit(&G) != cudaSuccess) return false;
+    if (std::get<6>(gp->key) && !G.specialised) {
+        // monomer-0 moves of linear chains exist in the specialised kernels
+        // only: a linear group without one refuses its jobs
+        for (SJob* j : gp->members) {
+            cudaFreeAsync(j->lat, gp->s);
+            cudaFreeAsync(j->rec, gp->s);
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->bytes_in_use -= j->bytes;
+            }
+            fail_job(s, j, ELP_ERR_ARG, "linear chains need a specialised kernel shape for their box");
+        }
+        gp->members.clear();
+        G.jobs.clear();
+        G.N.clear();
+    }
+    return true;
 }
 
 // End of a group's tick: count the steps of the jobs that ran, copy the
@@ -402,6 +420,7 @@ static void scheduler(elp_server* s)
                 s->fatal_msg = "group rebuild failed";
                 break;
             }
+            if (gp->members.empty()) continue;   // its jobs were refused
             gp->running = gp->members;
             if (elp_group_run(&gp->G, Q) != cudaSuccess || cudaEventRecord(gp->ev, gp->s) != cudaSuccess) {
                 s->fatal = ELP_ERR_CUDA;
@@ -498,7 +517,6 @@ extern "C" elp_status elp_server_submit(elp_server* s, const elp_job_spec* spec,
 {
     if (!s || !spec) return elp_fail(ELP_ERR_ARG, "null argument");
     if (nsteps < 1) return elp_fail(ELP_ERR_ARG, "a job needs at least one step");
-    if (spec->linear) return elp_fail(ELP_ERR_ARG, "the server runs ring melts; run linear chains with elp_create");
     const int64_t Q = s->o.quantum;
     if (nsteps % Q) return elp_fail(ELP_ERR_ARG, "steps must be a multiple of the quantum (%lld)", (long long)Q);
     if (dump_interval < 0 || (dump_interval && dump_interval % Q))

@@ -142,8 +142,11 @@ def test_linear_rejected_where_unsupported():
     with pytest.raises(elp.ElpError) as e:
         elp.Melt(L=32, N=50, linear=1, periodic=0, tile=(32, 16, 8))   # no specialised shape
     assert e.value.status == elp.ERR_ARG
+    # the serving loop takes linear jobs (tests/test_gpu_server.py); one whose
+    # box has no specialised shape finishes with ELP_ERR_ARG
     s = elp.Server(quantum=10)
-    with pytest.raises(elp.ElpError) as e:
-        s.submit(100, L=16, N=50, linear=1)
-    assert e.value.status == elp.ERR_ARG
+    jid = s.submit(100, L=32, N=50, linear=1, periodic=0, tile=(32, 16, 8))
+    s.drain(120)
+    r = s.poll()
+    assert len(r) == 1 and r[0]["id"] == jid and r[0]["status"] == elp.ERR_ARG
     s.close()

@@ -87,3 +87,27 @@ def test_rejects_bad_job_arguments():
     with pytest.raises(elp.ElpError):
         srv.submit(100, dump_interval=30, L=16, N=50)
     srv.close()
+
+
+def test_linear_chain_jobs_same_in_mix_and_plain(tmp_path):
+    """Linear-chain jobs (efpol_lin) share the server with rings in their own
+    groups and give the single-melt API's chains; a box without a
+    specialised kernel shape refuses them."""
+    lin = [dict(L=16, N=50, seed=21, linear=1), dict(L=64, N=200, seed=22, linear=1),
+           dict(L=48, N=100, seed=23, linear=1)]
+    steps = 200
+    srv = elp.Server(quantum=50)
+    ids = {}
+    for i, kw in enumerate(lin + JOBS[:2]):
+        ids[srv.submit(steps, dump_interval=100, dump_dir=str(tmp_path / f"j{i}"), **kw)] = kw
+        time.sleep(0.005)
+    bad = srv.submit(100, L=40, N=100, seed=24, linear=1)   # 40x20x20 tiles: generic kernel only
+    srv.drain(300)
+    res = {r["id"]: r for r in srv.poll()}
+    assert len(res) == len(ids) + 1
+    assert res[bad]["status"] == elp.ERR_ARG
+    for jid, kw in ids.items():
+        r = res[jid]
+        assert r["status"] == 0 and r["integrity"] == 0 and r["dumps"] == 2
+        assert r["checksum"] == plain_checksum(kw, steps), f"job {kw} differs from its single-melt run"
+    srv.close()
