@@ -61,3 +61,22 @@ def test_batch_load_and_fetch_roundtrip():
     s1, b1 = b.fetch(0)
     assert np.array_equal(s0, s1) and np.array_equal(b0, b1)
     assert b.info(0).step == 20
+
+
+def test_several_tiles_per_cta_give_the_same_bits():
+    """A group with more tiles than resident CTAs (12 melts x 16 tiles of
+    32x32x16 > 148) sweeps several tiles per CTA and step; every member still
+    equals its single run (16 tiles, one per CTA)."""
+    specs = [dict(L=64, N=200, seed=3000 + i, periodic=0, tile=(32, 32, 16)) for i in range(12)]
+    b = elp.Batch(specs)
+    b.init_melts()
+    b.run(12)
+    b.sync()
+    for j in (0, 5, 11):
+        m = elp.Melt(**specs[j])
+        m.init_melt()
+        m.run(12)
+        wa, ra = b.state(j)
+        wb, rb = m.state()
+        assert np.array_equal(wa, wb) and np.array_equal(ra, rb), f"member {j} differs from its single run"
+        assert b.check(j) == 0
