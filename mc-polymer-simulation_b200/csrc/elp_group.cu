@@ -90,8 +90,9 @@ cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int 
     G->stream = stream;
     G->d_table = d_table;
     G->d_error = d_error;
-    // step counter and the two counts of the grid barrier of tiled launches
-    cudaError_t e = cudaMalloc((void**)&G->d_ctr, 4 * sizeof(uint32_t));
+    // step counter and the two counts of the grid barrier of tiled launches,
+    // stream-ordered (a group created while others run does not stall them)
+    cudaError_t e = cudaMallocAsync((void**)&G->d_ctr, 4 * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(G->d_ctr, 0, 4 * sizeof(uint32_t), stream);
 }

@@ -99,6 +99,7 @@ struct elp_server {
     std::chrono::steady_clock::time_point t0;
     uint32_t* d_table = nullptr;
     uint32_t* d_err = nullptr;            // 64 groups x 4 words
+    uint32_t* h_err = nullptr;            // pinned: word 0 of each group's flags, copied at the end of its tick
     unsigned long long* d_acc = nullptr;  // accepted moves (all jobs together)
 
     std::mutex mu;
@@ -376,12 +377,8 @@ static bool complete_tick(elp_server* s, SGroup* gp, size_t gi)
     }
     gp->running.clear();
     // a domain whose monomer-0 runs outgrew its label table stops the server
-    uint32_t flag = 0;
-    if (cudaMemcpy(&flag, s->d_err + 4 * gi, sizeof(flag), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        s->fatal = ELP_ERR_CUDA;
-        s->fatal_msg = "cannot read device error flags";
-        return false;
-    }
+    // (the flags were copied to pinned memory behind the tick's launches)
+    const uint32_t flag = s->h_err[gi];
     if (flag) {
         s->fatal = ELP_ERR_STATE;
         s->fatal_msg = "a domain held more monomer-0 runs than its label table";
@@ -422,7 +419,10 @@ static void scheduler(elp_server* s)
             }
             if (gp->members.empty()) continue;   // its jobs were refused
             gp->running = gp->members;
-            if (elp_group_run(&gp->G, Q) != cudaSuccess || cudaEventRecord(gp->ev, gp->s) != cudaSuccess) {
+            if (elp_group_run(&gp->G, Q) != cudaSuccess ||
+                cudaMemcpyAsync(s->h_err + gi, s->d_err + 4 * gi, sizeof(uint32_t), cudaMemcpyDeviceToHost, gp->s) !=
+                    cudaSuccess ||
+                cudaEventRecord(gp->ev, gp->s) != cudaSuccess) {
                 s->fatal = ELP_ERR_CUDA;
                 s->fatal_msg = "launch failed";
                 break;
@@ -496,16 +496,27 @@ extern "C" elp_status elp_server_create(const elp_server_opts* opts, elp_server*
     s->o = *opts;
     s->t0 = std::chrono::steady_clock::now();
     if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, opts->device) != cudaSuccess) s->nsm = 148;
+    // jobs and snapshots come and go through cudaMallocAsync: keep freed
+    // blocks in this process's pool instead of unmapping them at every
+    // synchronisation and mapping them again for the next job
+    {
+        cudaMemPool_t pool;
+        uint64_t keep = UINT64_MAX;
+        if (cudaDeviceGetDefaultMemPool(&pool, opts->device) == cudaSuccess)
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     uint8_t tab[4096];
     elp_build_table(tab);
     if (cudaMalloc((void**)&s->d_table, 4096) != cudaSuccess || cudaMalloc((void**)&s->d_err, 64 * 16) != cudaSuccess ||
+        cudaMallocHost((void**)&s->h_err, 64 * sizeof(uint32_t)) != cudaSuccess ||
         cudaMalloc((void**)&s->d_acc, 8) != cudaSuccess ||
         cudaMemcpy(s->d_table, tab, 4096, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(s->d_err, 0, 64 * 16) != cudaSuccess || cudaMemset(s->d_acc, 0, 8) != cudaSuccess) {
-        cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc);
+        cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc); cudaFreeHost(s->h_err);
         delete s;
         return elp_fail(ELP_ERR_CUDA, "server set-up failed");
     }
+    memset(s->h_err, 0, 64 * sizeof(uint32_t));
     for (int i = 0; i < opts->io_threads; i++) s->io_threads.emplace_back(io_worker, s);
     s->sched = std::thread(scheduler, s);
     *out = s;
@@ -641,7 +652,7 @@ extern "C" void elp_server_destroy(elp_server* s)
         cudaStreamDestroy(gp->s);
         cudaEventDestroy(gp->ev);
     }
-    cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc);
+    cudaFree(s->d_table); cudaFree(s->d_err); cudaFree(s->d_acc); cudaFreeHost(s->h_err);
     for (SJob* j : s->finished) delete j;
     delete s;
 }

@@ -24,6 +24,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <atomic>
+
 #include "elp_device.cuh"
 #include "elp_kernels.h"
 
@@ -96,9 +98,9 @@ struct Shape {
     // threads of a warp take anchors from an 8 x 4 block of (y, z) rows
     static constexpr bool PERM = !PER && TY % 8 == 0 && TZ % 4 == 0 && AT % R == 0;
     // shared-memory word offsets: lattice, transition table (4096 bytes),
-    // neighbour offsets (27 x 16), colours, slot tables, slot count, the
-    // and the Philox words of the current and the next substep group when
-    // threads own < 4 anchors
+    // neighbour offsets (27 x 16), colours, slot tables, slot count, and the
+    // Philox words of the current and the next substep group when threads
+    // own < 4 anchors
     static constexpr int TABW = WORDS;
     static constexpr int OFFW = TABW + 1024;
     static constexpr int COLW = OFFW + 27 * 16;
@@ -603,8 +605,16 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
         // expected monomer-0 runs per domain must stay far inside the slot table
         const double m = l->max_runs_per_domain;
         if (!(PER ? m <= CAP : m + 8.0 * sqrt(m) + 16.0 <= CAP)) return cudaErrorNotSupported;
-        // set the shared-memory limit here, outside any stream capture
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
+        // set the shared-memory limit here, outside any stream capture, once
+        // per device (groups are committed often in the serving loop)
+        static std::atomic<uint32_t> done_devices{0};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        const uint32_t bit = dev < 32 ? 1u << dev : 0u;
+        if (e == cudaSuccess && !(bit && (done_devices.load() & bit))) {
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
+            if (e == cudaSuccess) done_devices.fetch_or(bit);
+        }
         if (e == cudaSuccess) {
             const_cast<Sweep2Launch*>(l)->threads_out = THREADS;
             const_cast<Sweep2Launch*>(l)->smem_out = SH::BYTES;
