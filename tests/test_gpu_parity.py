@@ -194,6 +194,21 @@ def test_l128_matches_replay():
     assert np.array_equal(w, r.lattice()) and np.array_equal(rec, r.records())
 
 
+@pytest.mark.parametrize("L,N,seed,spl,steps", [(128, 1000, 7, 20, 3), (256, 5000, 11, 2, 2)])
+def test_bench_workloads_match_replay_in_multi_step_launches(L, N, seed, spl, steps):
+    """The bench's headline and roofline melts at full size, run as the bench
+    runs them (several steps per cooperative launch), equal the replay."""
+    m = elp.Melt(L=L, N=N, seed=seed, steps_per_launch=spl)
+    m.init_melt()
+    r = replay_for(m, seed)
+    assert r.load(*efpol_start(L, N, m.P)) == 0
+    m.run(steps)
+    r.steps(steps)
+    w, rec = m.state()
+    assert np.array_equal(w, r.lattice()) and np.array_equal(rec, r.records())
+    assert m.check() == 0 and m.accepted() == r.accepted
+
+
 def test_bad_inputs_fail_cleanly(tmp_path):
     m = elp.Melt(L=16, N=50, seed=1)
     with pytest.raises(elp.ElpError) as e:
