@@ -60,6 +60,26 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def issue_ceiling(name, spl, ms_per_step, sm_mhz, sms_busy):
+    """The ceiling that binds this integer kernel: warp-instruction issue
+    (4 per cycle per SM).  Instructions per launch come from the committed ncu
+    capture of the same launch shape; frac is the issue rate achieved over the
+    step against the SMs that hold work at the sampled clock."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            inst = json.load(f).get(f"inst/{name}/spl{spl}")
+    except Exception:
+        inst = None
+    if not inst or not sm_mhz:
+        return None
+    per_step = inst / spl
+    achieved = per_step / (ms_per_step / 1e3)
+    peak = 4.0 * sms_busy * sm_mhz * 1e6
+    return {"bound": "issue", "warp_inst_per_step": per_step, "achieved": achieved, "peak": peak,
+            "unit": "warp inst/s", "frac": achieved / peak, "sms_with_work": sms_busy, "sm_mhz": sm_mhz}
+
+
 def profile_traffic(name, spl):
     """DRAM bytes per sweep launch of `spl` steps from the committed ncu
     summary, if one was captured for that launch shape."""
@@ -233,12 +253,16 @@ def run_elp(args, rank, world):
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    ic = issue_ceiling(args.workload, spl, ms_per_step, (clk_s or {}).get("sm_mhz"), min(sms, info.domains))
+    if ic:
+        line["issue_roofline"] = ic
 
     if rank == 0 and not args.no_extras:
         line["e2e"] = e2e_leg(elp, w, dev, args)
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps)
         if args.workload != "L256" and not args.no_l256:
-            line["L256"] = l256_leg(elp, torch, dev, flush, args)
+            line["L256"] = l256_leg(elp, torch, dev, flush, args, (clk_s or {}).get("sm_mhz"))
         if not args.no_batched:
             line["ensemble"] = batched_leg(elp, dev, args)
         if not args.no_served:
@@ -304,7 +328,7 @@ def timed_steps(m, torch, flush, dev, nsteps, spl=1):
     return times
 
 
-def l256_leg(elp, torch, dev, flush, args):
+def l256_leg(elp, torch, dev, flush, args, clock_mhz):
     w = WORKLOADS["L256"]
     M = w["N"] * npol(w)
     spl = max(1, args.l256_spl)
@@ -317,11 +341,16 @@ def l256_leg(elp, torch, dev, flush, args):
     ms = sum(times) / nsteps
     peak, _ = measured_peak()
     achieved = algo_bytes(w) / (ms / 1e3) / 1e9
-    return {"workload": f"ring melt L=256 N=5000 P=4027 seed=11, {spl} steps per sweep launch", "value": M / (ms / 1e3),
-            "unit": UNIT, "ms_per_step": ms, "steps": nsteps, "steps_per_launch": spl,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "algorithmic_bytes_per_launch": spl * algo_bytes(w),
-                         "traffic": profile_traffic("L256", spl)}}
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    out = {"workload": f"ring melt L=256 N=5000 P=4027 seed=11, {spl} steps per sweep launch", "value": M / (ms / 1e3),
+           "unit": UNIT, "ms_per_step": ms, "steps": nsteps, "steps_per_launch": spl,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "algorithmic_bytes_per_launch": spl * algo_bytes(w),
+                        "traffic": profile_traffic("L256", spl)}}
+    ic = issue_ceiling("L256", spl, ms, clock_mhz, min(sms, m.info().domains))
+    if ic:
+        out["issue_roofline"] = ic
+    return out
 
 
 # ---- batched ensemble (512 replicas) ------------------------------------------
