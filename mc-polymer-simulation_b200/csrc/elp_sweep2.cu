@@ -668,6 +668,7 @@ extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
                          : launch2<X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_, false>(l, s);
     SHAPE(32, 32, 32, 0, 16, 40, 1364, 1792, 2, 1024, 1)
     SHAPE(32, 32, 16, 0, 16, 40, 1364, 1024, 1, 1024, 1)
+    SHAPE(32, 16, 16, 0, 16, 40, 724, 1024, 1, 512, 2)
     SHAPE(16, 16, 16, 0, 16, 24, 444, 512, 1, 256, 4)
     SHAPE(48, 24, 24, 0, 16, 56, 1456, 2048, 2, 864, 1)
     SHAPE(16, 16, 16, 1, 16, 16, 256, 2048, 1, 256, 1)

@@ -40,6 +40,7 @@ CASES = [
     (32, 100, dict(periodic=0, tile=(16, 16, 16)), 8),      # tiled with origin shifts
     (64, 200, dict(periodic=0, tile=(32, 32, 32)), 3),
     (48, 100, dict(periodic=0, tile=(48, 24, 24)), 3),
+    (64, 150, dict(periodic=0, tile=(32, 16, 16)), 3),      # two CTAs per SM
 ]
 
 

@@ -41,6 +41,7 @@ CASES = [
     (32, 100, dict(periodic=0, tile=(16, 16, 16)), 8),      # tiled with origin shifts
     (64, 200, dict(periodic=0, tile=(32, 32, 32)), 3),
     (48, 100, dict(periodic=0, tile=(48, 24, 24)), 3),
+    (64, 150, dict(periodic=0, tile=(32, 16, 16)), 3),      # two CTAs per SM
     (32, 50, dict(periodic=0, tile=(32, 16, 8)), 6),
 ]
 
@@ -241,6 +242,7 @@ def test_bad_inputs_fail_cleanly(tmp_path):
 @pytest.mark.parametrize("L,N,kw", [(16, 50, dict()), (24, 60, dict()), (32, 100, dict()),
                                      (64, 200, dict(periodic=0, tile=(32, 32, 32))),
                                      (64, 200, dict(periodic=0, tile=(32, 32, 16))),
+                                     (64, 200, dict(periodic=0, tile=(32, 16, 16))),
                                      (32, 100, dict(periodic=0, tile=(16, 16, 16))),
                                      (48, 100, dict(periodic=0, tile=(48, 24, 24)))])
 def test_specialised_kernels_equal_generic(L, N, kw):
