@@ -75,7 +75,9 @@ static int pick_geometry(const elp_job_spec* s, elp_geometry* g)
     static const int cand[][3] = {{32, 32, 32}, {48, 24, 24}, {32, 32, 16}, {24, 24, 24}, {32, 16, 16},
                                   {16, 16, 16}, {40, 20, 20}, {20, 20, 20}, {16, 16, 8}};
     int first = 0;
-    if (L == 128) first = 2;  // 128 domains of 32x32x16 rather than 64 of 32^3
+    // L = 128: 256 domains of 32x32x16 / 2 at two CTAs per SM rather than 128
+    // of 32x32x16 on 128 of the SMs (more attempted and more accepted moves/s)
+    if (L == 128) first = 4;
     for (size_t i = (size_t)first; i < sizeof(cand) / sizeof(cand[0]); i++) {
         g->tx = cand[i][0]; g->ty = cand[i][1]; g->tz = cand[i][2];
         if (L % g->tx || L % g->ty || L % g->tz) continue;
