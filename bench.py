@@ -227,6 +227,15 @@ def run_elp(args, rank, world):
     value = world * args.steps * M / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
     assert m.check() == 0, "integrity check failed after the timed run"
+    # the same melt with one kernel launch per MC step (every launch flushed
+    # from L2 first), beside the multi-step launches of the headline
+    one = None
+    if args.one_step_launches > 0 and not args.no_extras:
+        ot = timed_steps(m, torch, flush, dev, args.one_step_launches, 1)
+        one_ms = max_over_ranks(sum(ot), world) / len(ot)
+        one = {"ms_per_step": one_ms, "value": world * M / (one_ms / 1e3), "unit": UNIT, "launches": len(ot),
+               "l2": "flushed before every launch"}
+        assert m.check() == 0, "integrity check failed after the one-step launches"
 
     peak, peak_kind = measured_peak()
     achieved = algo_bytes(w) / (ms_per_step / 1e3) / 1e9
@@ -250,6 +259,8 @@ def run_elp(args, rank, world):
                      "traffic": tr},
         "gpu_launches": len(times),
     }
+    if one:
+        line["one_step_per_launch"] = one
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
@@ -301,10 +312,28 @@ def e2e_leg(elp, w, dev, args):
         cycle(step)
         step += interval
     dt = time.perf_counter() - t0
+    # where a cycle's time goes: a few more cycles (not in the number above),
+    # with a synchronisation after elp_run so that each part is closed
+    parts = {"load_chains": [], "run": [], "fetch_chains": []}
+    for _ in range(5):
+        t1 = time.perf_counter()
+        m.load_chains(start, bonds, step)
+        t2 = time.perf_counter()
+        m.run(interval)
+        m.sync()
+        t3 = time.perf_counter()
+        m.fetch(start, bonds)
+        t4 = time.perf_counter()
+        step += interval
+        parts["load_chains"].append(t2 - t1)
+        parts["run"].append(t3 - t2)
+        parts["fetch_chains"].append(t4 - t3)
     assert m.check() == 0
     return {"value": reps * interval * N * P / dt, "unit": UNIT,
             "h2d_bytes_per_step": 12 * P + N * P, "d2h_bytes_per_step": 12 * P + N * P,
             "steps_per_call": interval, "calls_timed": reps,
+            "ms_per_call": 1e3 * dt / reps,
+            "parts_ms_median": {k: 1e3 * sorted(v)[len(v) // 2] for k, v in parts.items()},
             "path": "elp_load_chains(host) + elp_run(interval) + elp_fetch_chains(host), wall clock"}
 
 
@@ -531,6 +560,8 @@ def main():
     ap.add_argument("--l256-spl", type=int, default=10, help="MC steps per sweep launch of the L=256 leg")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--ref-steps", type=int, default=8)
+    ap.add_argument("--one-step-launches", type=int, default=100,
+                    help="launches of one MC step each, timed after the headline launches (0: none)")
     ap.add_argument("--e2e-interval", type=int, default=100)
     ap.add_argument("--e2e-reps", type=int, default=20)
     ap.add_argument("--no-extras", action="store_true")

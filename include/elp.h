@@ -115,7 +115,10 @@ elp_status elp_sync(elp_ctx* ctx);
 
 /* Rebuild the rings on the device and copy them to host buffers
  * start[3*P] (int32) and bonds[P*N] (uint8).  Blocking.  Returns
- * ELP_ERR_INTEGRITY if a ring cannot be walked. */
+ * ELP_ERR_STATE if an earlier launch reported an error (as elp_sync), else
+ * ELP_ERR_INTEGRITY if a ring cannot be walked; on either error the
+ * buffers' contents are unspecified.  With pinned buffers the copies run
+ * asynchronously behind the walk, itself queued behind the steps. */
 elp_status elp_fetch_chains(elp_ctx* ctx, int32_t* start, uint8_t* bonds);
 
 /* Write the current state as a TUV file, byte-compatible with the

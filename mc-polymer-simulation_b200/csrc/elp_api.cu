@@ -148,12 +148,12 @@ extern "C" elp_status elp_load_chains(elp_ctx* c, const int32_t* start, const ui
     if (!c || !start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
     ELP_CUDA_TRY(cudaSetDevice(c->device));
     // the lattice is rebuilt in place on the device: until that succeeds the
-    // context holds no configuration
+    // context holds no configuration.  The step is queued ahead of the build,
+    // whose status read-back is the call's one synchronisation.
     c->loaded = 0;
+    ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, step));
     elp_status st = elp_build_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, start, bonds, &c->wb, c->stream);
     if (st) return st;
-    ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, step));
-    ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->loaded = 1;
     return ELP_OK;
 }
@@ -241,9 +241,12 @@ extern "C" elp_status elp_fetch_chains(elp_ctx* c, int32_t* start, uint8_t* bond
     if (!c || !start || !bonds) return elp_fail(ELP_ERR_ARG, "null argument");
     if (!c->loaded) return elp_fail(ELP_ERR_STATE, "no configuration loaded");
     ELP_CUDA_TRY(cudaSetDevice(c->device));
-    elp_status st = elp_device_errors(error_flags(c), c->stream);
-    if (st) return st;
-    return elp_fetch_rings(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, start, bonds, c->stream);
+    // the walk is queued straight behind the steps (no host round trip in
+    // between); the launches' error flags are read after it and take
+    // precedence over the walk's status
+    elp_status st = elp_fetch_rings(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, start, bonds, c->stream);
+    elp_status fl = elp_device_errors(error_flags(c), c->stream);
+    return fl ? fl : st;
 }
 
 extern "C" elp_status elp_observe(elp_ctx* c, double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist,

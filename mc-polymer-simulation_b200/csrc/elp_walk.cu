@@ -17,62 +17,134 @@
 
 namespace elp {
 
-__device__ __forceinline__ uint32_t step_site(uint32_t cur, uint32_t b, int L)
-{
-    int t = (int)(cur % (uint32_t)L), u = (int)((cur / (uint32_t)L) % (uint32_t)L), v = (int)(cur / ((uint32_t)L * L));
-    t += elp_bt(b); u += elp_bu(b); v += elp_bv(b);
-    t += t < 0 ? L : 0; t -= t >= L ? L : 0;
-    u += u < 0 ? L : 0; u -= u >= L ? L : 0;
-    v += v < 0 ? L : 0; v -= v >= L ? L : 0;
-    return (uint32_t)t + (uint32_t)L * ((uint32_t)u + (uint32_t)L * (uint32_t)v);
-}
+// One bond step on the periodic box, in coordinates (no division).
+struct Pos {
+    int t, u, v;
+    __device__ __forceinline__ Pos step(uint32_t b, int L) const
+    {
+        int nt = t + elp_bt(b), nu = u + elp_bu(b), nv = v + elp_bv(b);
+        nt += nt < 0 ? L : 0; nt -= nt >= L ? L : 0;
+        nu += nu < 0 ? L : 0; nu -= nu >= L ? L : 0;
+        nv += nv < 0 ? L : 0; nv -= nv >= L ? L : 0;
+        return Pos{nt, nu, nv};
+    }
+    __device__ __forceinline__ uint32_t index(int L) const
+    {
+        return (uint32_t)t + (uint32_t)L * ((uint32_t)u + (uint32_t)L * (uint32_t)v);
+    }
+};
 
+// Writes one chain's bond bytes [lo, hi) of a byte array in increasing order:
+// eight bytes per store where the aligned 8-byte word lies inside [lo, hi),
+// byte by byte in the words at either end, which the neighbouring chains
+// (other threads) share.  Bytes skipped between two puts are zero.
+struct BondWriter {
+    uint8_t* base;
+    size_t lo, hi;   // the chain's bytes
+    size_t w;        // current word (byte offset, multiple of 8)
+    uint64_t acc;    // its bytes so far
+    ELP_HD void init(uint8_t* b, size_t l, size_t h)
+    {
+        base = b; lo = l; hi = h; w = l & ~(size_t)7; acc = 0;
+    }
+    ELP_HD void flush()
+    {
+        if (w >= lo && w + 8 <= hi) {
+            *reinterpret_cast<uint64_t*>(base + w) = acc;
+        } else {
+            for (int k = 0; k < 8; k++)
+                if (w + k >= lo && w + k < hi) base[w + k] = (uint8_t)(acc >> (8 * k));
+        }
+    }
+    // byte v at offset g: lo <= g < hi, and g above every earlier put
+    ELP_HD void put(size_t g, uint8_t v)
+    {
+        const size_t gw = g & ~(size_t)7;
+        while (w < gw) { flush(); w += 8; acc = 0; }
+        acc |= (uint64_t)v << (8 * (g & 7));
+    }
+    // the current word and zero words up to hi
+    ELP_HD void finish()
+    {
+        for (;;) {
+            flush();
+            w += 8; acc = 0;
+            if (w >= hi) break;
+        }
+    }
+};
+
+// One warp per chain.  The walk is a chain of dependent loads, one per run,
+// so each round trip fetches the words of the next run's site and of its 16
+// bond-code neighbours (lane j: the site one step of code j away, lane 0 the
+// site itself): the run after next is then among them, and a round trip
+// advances two runs.  All lanes follow the same (uniform) walk; lane 0 writes
+// the results.
 __global__ void walk_kernel(WalkArgs a)
 {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.P) return;
+    const int lane = threadIdx.x & 31;
+    const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    if (p >= a.P) return;   // p is the same in the whole warp
     const int L = a.L, N = a.N;
     const size_t S = (size_t)L * L * L;
     uint32_t site = a.rec[ELP_REC_WORDS * p], cnt = a.rec[ELP_REC_WORDS * p + 1], off = a.rec[ELP_REC_WORDS * p + 2];
     int bad = 0;
     if (site >= S || off >= cnt || cnt == 0 || (a.linear && off != 0)) bad = 1;
-    uint32_t w = bad ? 0 : a.lat[site];
+    Pos cur{(int)(site % (uint32_t)L), (int)((site / (uint32_t)L) % (uint32_t)L), (int)(site / ((uint32_t)L * L))};
+    // words around the first site (in bounds: a step of any code wraps)
+    uint32_t v = (!bad && lane < 16) ? a.lat[cur.step((uint32_t)lane, L).index(L)] : 0u;
+    const uint32_t w = __shfl_sync(0xffffffffu, v, 0);
+    bool spec = true;   // lane j holds the word one step of code j from cur
     if (!bad && (!(w & ELP_LBIT) || (w >> 5) != (uint32_t)p)) bad = 1;
-    if (bad) { a.status[p] = 4; return; }
-    if (a.start) {
-        a.start[3 * p] = (int32_t)(site % (uint32_t)L);
-        a.start[3 * p + 1] = (int32_t)((site / (uint32_t)L) % (uint32_t)L);
-        a.start[3 * p + 2] = (int32_t)(site / ((uint32_t)L * L));
+    if (bad) {
+        if (lane == 0) a.status[p] = 4;
+        return;
     }
-    uint8_t* b = a.bonds ? a.bonds + (size_t)p * N : nullptr;
+    if (a.start && lane == 0) {
+        a.start[3 * p] = cur.t;
+        a.start[3 * p + 1] = cur.u;
+        a.start[3 * p + 2] = cur.v;
+    }
+    BondWriter bw;
+    const bool wr = a.bonds != nullptr && lane == 0;
+    if (wr) bw.init(a.bonds, (size_t)p * N, (size_t)p * N + N);
     long i = 0;
-    uint32_t here = cnt - off, cur = site;
+    uint32_t here = cnt - off, ci = site, wc = w;
     unsigned long long runs = 0;
     for (;;) {
-        uint32_t bo = a.lat[cur] & 15;
+        const uint32_t bo = wc & 15;
         const bool end = a.linear && bo == 15;   // last run of a linear chain
         if (!(elp_valid_bond(bo) || end) || i + (long)here > (long)N) { bad = 1; break; }
-        if (b) {
-            for (uint32_t k = 0; k + 1 < here; k++) b[i + k] = 0;
-            b[i + here - 1] = (uint8_t)bo;
-        }
+        if (wr) bw.put((size_t)p * N + (size_t)(i + here - 1), (uint8_t)bo);
         i += here;
         runs++;
-        if (a.visit) atomicAdd(&a.visit[cur], 1u);
+        if (a.visit && lane == 0) atomicAdd(&a.visit[ci], 1u);
         if (end) break;
-        cur = step_site(cur, bo, L);
-        uint32_t wn = a.lat[cur];
+        const Pos nxt = cur.step(bo, L);
+        uint32_t wn;
+        if (spec) {
+            wn = __shfl_sync(0xffffffffu, v, (int)bo);
+            spec = false;
+        } else {
+            v = lane < 16 ? a.lat[nxt.step((uint32_t)lane, L).index(L)] : 0u;
+            wn = __shfl_sync(0xffffffffu, v, 0);
+            spec = true;
+        }
+        cur = nxt;
+        ci = nxt.index(L);
         if (!wn) { bad = 1; break; }
-        if (cur == site) break;
+        if (ci == site) break;
         if (wn & ELP_LBIT) { bad = 1; break; }
         here = wn >> ELP_CSHIFT;
         if (here == 0 || runs >= (unsigned long long)N) { bad = 1; break; }
+        wc = wn;
     }
     if (!bad && i + (long)off != N) bad = 1;
-    if (!bad && b)
-        for (uint32_t k = 0; k < off; k++) b[i + k] = 0;
-    a.status[p] = bad ? 4 : 0;
-    if (a.counters) atomicAdd(&a.counters[0], runs);
+    if (wr) bw.finish();   // the off monomers ahead of monomer 0 in its run: zeros
+    if (lane == 0) {
+        a.status[p] = bad ? 4 : 0;
+        if (a.counters) atomicAdd(&a.counters[0], runs);
+    }
 }
 
 __global__ void scan_kernel(WalkArgs a)
@@ -119,7 +191,8 @@ __global__ void scan_kernel(WalkArgs a)
 extern "C" cudaError_t elp_launch_walk(const WalkArgs* a, cudaStream_t s)
 {
     if (a->P <= 0) return cudaSuccess;
-    elp::walk_kernel<<<(a->P + 127) / 128, 128, 0, s>>>(*a);
+    // one warp per chain, four chains per block
+    elp::walk_kernel<<<(unsigned)(((size_t)a->P * 32 + 127) / 128), 128, 0, s>>>(*a);
     return cudaGetLastError();
 }
 
