@@ -332,6 +332,7 @@ def e2e_leg(elp, w, dev, args):
     return {"value": reps * interval * N * P / dt, "unit": UNIT,
             "h2d_bytes_per_step": 12 * P + N * P, "d2h_bytes_per_step": 12 * P + N * P,
             "steps_per_call": interval, "calls_timed": reps,
+            "bytes_per": f"call cycle (load, {interval} MC steps, fetch): the chains go in and come back once per cycle",
             "ms_per_call": 1e3 * dt / reps,
             "parts_ms_median": {k: 1e3 * sorted(v)[len(v) // 2] for k, v in parts.items()},
             "path": "elp_load_chains(host) + elp_run(interval) + elp_fetch_chains(host), wall clock"}
