@@ -11,7 +11,9 @@ Default workload: the single large ring melt L=128, N=1000, density 1.2
 kernel launch (a cooperative launch whose CTAs meet at a grid barrier between
 steps; the same bits as one step per launch).  The lattice (8 MB) is smaller
 than L2, so L2 is flushed before every timed launch (a 256 MB write outside
-the timed events).  Extra legs on rank 0: the L=256, N=5000 melt (roofline
+the timed events).  After the timed launches the same melt runs
+--one-step-launches launches of one step each (`one_step_per_launch` in the
+line: one kernel per MC step).  Extra legs on rank 0: the L=256, N=5000 melt (roofline
 configuration), the reference CPU efpol timed on this host, and the
 end-to-end path through the C ABI with host buffers.
 
