@@ -86,7 +86,9 @@ __global__ void build_kernel(BuildArgs a)
     int after = __shfl_down_sync(0xffffffffu, sm, 1);
     if (lane == 31) after = INT_MAX;
     const int first_all = __shfl_sync(0xffffffffu, sm, 0);
-    int t = t0 + it - dt, u = u0 + iu - du, v = v0 + iv - dv;   // position of monomer m0
+    // position of monomer m0 in the box; each bond then moves it by at most
+    // one site per axis, wrapped without a division
+    int t = wrap(t0 + it - dt, L), u = wrap(u0 + iu - du, L), v = wrap(v0 + iv - dv, L);
     int status = 0;
     for (int m = m0; m < m1; m++) {
         const uint32_t prev = b[m == 0 ? N - 1 : m - 1];
@@ -96,8 +98,7 @@ __global__ void build_kernel(BuildArgs a)
             if (e == m1) e = (after != INT_MAX) ? after : first_all + N;   // it ends in a later chunk, or wraps
             const int len = e - m + 1;
             const uint32_t bo = b[e % N];
-            const uint32_t site =
-                (uint32_t)wrap(t, L) + (uint32_t)L * ((uint32_t)wrap(u, L) + (uint32_t)L * (uint32_t)wrap(v, L));
+            const uint32_t site = (uint32_t)t + (uint32_t)L * ((uint32_t)u + (uint32_t)L * (uint32_t)v);
             const int off0 = (N - m) % N;
             const bool head = off0 < len;   // this run holds monomer 0
             const uint32_t word = head ? (bo | ELP_LBIT | ((uint32_t)p << 5)) : (bo | ((uint32_t)len << ELP_CSHIFT));
@@ -108,6 +109,9 @@ __global__ void build_kernel(BuildArgs a)
         }
         const uint32_t bm = b[m];
         t += elp_bt(bm); u += elp_bu(bm); v += elp_bv(bm);
+        t += t < 0 ? L : 0; t -= t >= L ? L : 0;
+        u += u < 0 ? L : 0; u -= u >= L ? L : 0;
+        v += v < 0 ? L : 0; v -= v >= L ? L : 0;
     }
     if (__any_sync(0xffffffffu, status)) {
         if (lane == 0) a.status[p] = 3;

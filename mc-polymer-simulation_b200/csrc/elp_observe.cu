@@ -52,6 +52,9 @@ __global__ void observe_kernel(ObsArgs a)
         int dt = 0, du = 0, dv = 0;    // position of the current run relative to monomer 0's site
         long mono = 0;
         uint32_t here = cnt - off, cur = site, len = cnt;
+        // the current run's site in box coordinates, stepped without a division
+        int t = (int)(site % (uint32_t)L), u = (int)((site / (uint32_t)L) % (uint32_t)L),
+            v = (int)(site / ((uint32_t)L * L));
         while (!bad) {
             const uint32_t bo = a.lat[cur] & 15;
             const bool end = a.linear && bo == 15;   // last run of a linear chain
@@ -66,8 +69,6 @@ __global__ void observe_kernel(ObsArgs a)
             atomicAdd(&hist[(len < (uint32_t)a.nbins ? len : (uint32_t)a.nbins) - 1], 1ull);
             if (end) break;
             // next run
-            int t = (int)(cur % (uint32_t)L), u = (int)((cur / (uint32_t)L) % (uint32_t)L),
-                v = (int)(cur / ((uint32_t)L * L));
             t += elp_bt(bo); u += elp_bu(bo); v += elp_bv(bo);
             dt += elp_bt(bo); du += elp_bu(bo); dv += elp_bv(bo);
             t += t < 0 ? L : 0; t -= t >= L ? L : 0;
