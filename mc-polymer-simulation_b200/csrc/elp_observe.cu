@@ -1,7 +1,7 @@
 // elp_observe.cu -- in-situ observables of a melt, computed on the device.
 //
-// One thread per ring walks the ring from monomer 0's run (as walk_kernel
-// does) and accumulates exact integer sums over its monomers, positions
+// One thread per ring walks the ring from monomer 0's run (walk_kernel
+// follows the same runs, one warp per ring) and accumulates exact integer sums over its monomers, positions
 // taken relative to monomer 0's site and unwrapped along the ring:
 //   St, Su, Sv    sums of the lattice coordinates (t, u, v)
 //   Sq            sum of x^2 + y^2 + z^2 with x = t+u-v, y = t-u, z = v
