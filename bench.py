@@ -416,6 +416,34 @@ def ensemble_mix(n=512, first_seed=1000, density=1.2):
     return out
 
 
+def cpu_ensemble(mix, target_moves=1e8, max_procs=None):
+    """The reference efpol on the ensemble's members it can run (L a power of
+    two: 16, 32, 64), one process per host core at once, each a bounded sample
+    of about target_moves attempted moves; the aggregate is the sum of the
+    processes' own rates (they run concurrently)."""
+    ref = os.path.join(REPO, "oracle", "_ref", "ref_bench")
+    kind = "reference"
+    if not os.path.exists(ref):
+        ref = os.path.join(REPO, "oracle", "efpol_port")
+        kind = "port"
+        if not os.path.exists(ref):
+            subprocess.run(["make", "-C", os.path.join(REPO, "oracle")], check=True, stdout=subprocess.DEVNULL)
+    members = [m for m in mix if m["L"] in (16, 32, 64)]
+    nproc = min(len(members), max_procs or os.cpu_count() or 1)
+    members = members[:nproc]
+    procs = []
+    for m in members:
+        M = m["N"] * max(1, int(m["density"] * m["L"] ** 3 / m["N"] + 0.5))
+        steps = max(10, int(target_moves / M))
+        procs.append(subprocess.Popen([ref, str(m["L"]), str(m["N"]), str(m["density"]), str(m["seed"]), str(steps)],
+                                      stdout=subprocess.PIPE, text=True))
+    outs = [json.loads(p.communicate()[0].strip().splitlines()[-1]) for p in procs]
+    rate = sum(o["moves"] / o["seconds"] for o in outs)
+    return {"value": rate, "unit": UNIT, "cores": nproc, "kind": kind,
+            "sample": f"the first {nproc} members with L in {{16,32,64}} (efpol rounds L up to a power of two, so "
+                      f"L=24/48 do not run), about {target_moves:.0e} attempted moves each, one process per core"}
+
+
 def batched_leg(elp, dev, args):
     mix = ensemble_mix(args.replicas)
     tuned = {}
@@ -459,7 +487,8 @@ def batched_leg(elp, dev, args):
             "batched": {"value": batched, "unit": UNIT, "ms": bms},
             "plain": {"value": plain, "unit": UNIT, "ms": pms, "how": "each replica alone, same specs, sequential"},
             "speedup": batched / plain, "batched_equals_plain_bits": same,
-            "replicas_compared": len(check_idx), "autotuned_geometry": geoms}
+            "replicas_compared": len(check_idx), "autotuned_geometry": geoms,
+            "cpu_reference": cpu_ensemble(mix)}
 
 
 # ---- served stream ------------------------------------------------------------
