@@ -46,3 +46,14 @@ def test_reference_arm_under_two_ranks():
     lines = [x for x in out.stdout.splitlines() if x.strip().startswith("{")]
     assert len(lines) == 1
     check_line(lines[0], 2)
+
+
+def test_cpu_ensemble_leg_runs_the_power_of_two_members():
+    sys.path.insert(0, REPO)
+    import bench
+    mix = bench.ensemble_mix(64)
+    out = bench.cpu_ensemble(mix, target_moves=2e5, max_procs=4)
+    assert out["unit"] == "moves/s" and out["value"] > 0
+    assert out["kind"] in ("reference", "port") and 1 <= out["cores"] <= 4
+    assert all(m["L"] in (16, 24, 32, 48, 64) for m in mix)
+    assert sum(1 for m in mix if m["L"] in (16, 32, 64)) >= out["cores"]
