@@ -81,7 +81,7 @@ __device__ __forceinline__ void grid_exit(uint32_t* bar)
     }
 }
 
-template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K>
+template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int MINB>
 struct Shape {
     static constexpr int R = TY * TZ;
     static constexpr int A = R * (TX / NC);   // anchors per substep
@@ -99,8 +99,7 @@ struct Shape {
     static constexpr bool PERM = !PER && TY % 8 == 0 && TZ % 4 == 0 && AT % R == 0;
     // shared-memory word offsets: lattice, transition table (4096 bytes),
     // neighbour offsets (27 x 16), colours, slot tables, slot count, and the
-    // Philox words of the current and the next substep group when threads
-    // own < 4 anchors
+    // Philox words when threads own < 4 anchors
     static constexpr int TABW = WORDS;
     static constexpr int OFFW = TABW + 1024;
     static constexpr int COLW = OFFW + 27 * 16;
@@ -110,8 +109,14 @@ struct Shape {
     static constexpr int NSLW = SSIW + CAP;
     static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
     static constexpr int RNDW = (HTABW + 64 + 4) & ~3;
-    // two buffers of Philox words: the next group's are drawn during this one
-    static constexpr int TOTW = RNDW + (K < 4 ? 8 * G : 0);
+    static constexpr int NG = 2 * NC / 4;     // substep groups per step
+    static constexpr size_t bytes_with(int groups) { return (size_t)(RNDW + (K < 4 ? groups * G * 4 : 0)) * 4; }
+    // Philox words of threads that own < 4 anchors: in tiled domains, where
+    // MINB CTAs still fit on an SM (228 KB, 1 KB reserved per CTA), all NG
+    // groups of the step, drawn while the tile loads (PRE); else two buffers,
+    // the next group's drawn during this one
+    static constexpr bool PRE = !PER && K < 4 && (size_t)MINB * (bytes_with(NG) + 1024) <= 233472;
+    static constexpr int TOTW = RNDW + (K < 4 ? (PRE ? NG : 2) * G * 4 : 0);
     static constexpr size_t BYTES = (size_t)TOTW * 4;
     static_assert(PER || (SX % 4 == 0 && SXY % 4 == 0 && SX >= SPAN + 1 && SXY >= SX * (TY + 2)),
                   "tiled rows: 16-byte aligned, room for the span and the halo word before it");
@@ -302,7 +307,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB, bool LIN>
 __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 {
-    using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K>;
+    using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, MINB>;
     static_assert(K == 1 || K == 2 || K == 4, "anchors per thread");
     static_assert(SH::A % 4 == 0 && SH::AT <= THREADS, "threads");
     static_assert(CAP <= 2048, "slot numbers are 11 bits");
@@ -453,6 +458,11 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                         int gx = xa + 4 * c; gx -= gx >= L ? L : 0;
                         cp_async16(S + SH::OX + SX * y + SXY * z + 4 * c, lat + (uint32_t)(gx + L * (gy + L * gz)));
                     }
+                    // the step's Philox words while the rows are in flight
+                    // (the same counters as the two-buffer schedule draws)
+                    if (SH::PRE)
+                        for (int i = tid; i < SH::NG * SH::G; i += THREADS)
+                            rnd[i] = philox(make_uint4(t, (uint32_t)d, (uint32_t)(i / SH::G), (uint32_t)(i % SH::G)), key);
                     cp_async_wait_all();
                     __syncthreads();
                     // span words outside the tile become halo words; with many
@@ -502,7 +512,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                     }
                 }
             }
-            if (K < 4 && tid < SH::G) rnd[tid] = philox(make_uint4(t, (uint32_t)d, 0u, (uint32_t)tid), key);
+            if (K < 4 && !SH::PRE && tid < SH::G) rnd[tid] = philox(make_uint4(t, (uint32_t)d, 0u, (uint32_t)tid), key);
             if (tid < (2 * NC + 3) / 4) {
                 const uint4 cw = philox(make_uint4(t, (uint32_t)d, (uint32_t)tid | ELP_STREAM_COLOUR, 0), key);
                 col[4 * tid + 0] = 4 * bounded(cw.x, NC);   // colours in bytes of x offset
@@ -522,6 +532,8 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 uint4 rw = make_uint4(0, 0, 0, 0);
                 if (K == 4) {
                     if (active) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                } else if (SH::PRE) {
+                    if (active) rw = rnd[(k >> 2) * SH::G + gq];
                 } else {
                     // this group's words were drawn during the previous one (or
                     // before the first); G threads now draw the next group's
@@ -599,7 +611,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB, bool LIN>
 static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 {
-    using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K>;
+    using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, MINB>;
     auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, THREADS, MINB, LIN>;
     if (l->check_only) {
         // expected monomer-0 runs per domain must stay far inside the slot table
