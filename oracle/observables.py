@@ -9,8 +9,12 @@ project's output and from the reference efpol's output are comparable:
 * centre of mass per chain (ComputeCMS, mode_compute.c:205-217)
 * stored-length fraction per chain: share of monomers that sit on the same
   site as their successor (ComputeSL, mode_compute.c:145-153)
-* centre-of-mass mean-square displacement with the melt's mean drift removed
-  (AddCMS, mode_compute.c:548-569)
+* centre-of-mass mean-square displacement (AddCMS, mode_compute.c:548-569):
+  the reference removes the melt's mean drift using avg_pos.dat, which its
+  first pass over a sample only writes (AddAvgPos, :244-252; mode_init.c:389),
+  so the cmsdif_raw.dat of that pass holds the MSD without drift removal.
+  Both forms are here (``drift``).  Pinned to the reference's lowm_modes
+  output by tests/test_observables_ref.py.
 * stored-length histogram: number of monomers per occupied site.  The
   reference has no such histogram; it is defined here from the same run
   lengths for both engines.
@@ -129,14 +133,16 @@ def cms_tuv(start: np.ndarray, bonds: np.ndarray) -> np.ndarray:
     return unwrapped_tuv(start, bonds).mean(axis=1)
 
 
-def cms_msd(cms_t: np.ndarray, lags) -> np.ndarray:
+def cms_msd(cms_t: np.ndarray, lags, drift: bool = True) -> np.ndarray:
     """Mean-square displacement of chain centres of mass (xyz units) at the
-    given lags (in dump intervals), melt drift removed.  cms_t: (T, P, 3) in
-    continuous lattice units."""
+    given lags (in dump intervals), averaged over every time origin and
+    chain; with ``drift`` the melt's mean displacement over the lag is
+    removed first.  cms_t: (T, P, 3) in continuous lattice units."""
     xyz = to_xyz(cms_t)
     res = []
     for lag in lags:
         d = xyz[lag:] - xyz[:-lag] if lag > 0 else np.zeros_like(xyz)
-        d = d - d.mean(axis=1, keepdims=True)
+        if drift:
+            d = d - d.mean(axis=1, keepdims=True)
         res.append((d ** 2).sum(axis=2).mean())
     return np.array(res)

@@ -94,6 +94,9 @@ int  orc_replay_export(const orc_replay* r, int32_t* start, uint8_t* bonds);
 void orc_replay_steps(orc_replay* r, long nsteps);
 /* Linear chains (set before load). */
 void orc_replay_set_linear(orc_replay* r, int linear);
+/* Take a state as it stands (site words L^3, records 4*P, in the layout
+ * above) at absolute step `step`: e.g. a melt the GPU has relaxed. */
+void orc_replay_set_state(orc_replay* r, const uint32_t* lat, const uint32_t* rec, uint64_t step);
 
 #ifdef __cplusplus
 }

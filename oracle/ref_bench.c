@@ -7,7 +7,10 @@
  * and times the reference's own DoMCStep (cpupol/efpol_lib.c:122) with a
  * monotonic clock, excluding file output and the trailing sleep(1).
  *
- * usage: ref_bench L N density seed steps
+ * usage: ref_bench L N density seed steps [tuv]
+ * With a TUV file the melt is read by the reference's own ReadLatticeFile
+ * (cpupol/efpol_io.c:3-47) instead of built by CreatePolymers: the timed
+ * steps then start from that configuration (e.g. a relaxed melt).
  * Prints {"moves_per_s":..,"seconds":..,"moves":..,"integrity":..}.
  */
 #define IS_MAIN
@@ -16,7 +19,7 @@
 
 int main(int argc, char** argv)
 {
-    if (argc < 6) { fprintf(stderr, "usage: %s L N density seed steps\n", argv[0]); return 1; }
+    if (argc < 6) { fprintf(stderr, "usage: %s L N density seed steps [tuv]\n", argv[0]); return 1; }
     int L = atoi(argv[1]), N = atoi(argv[2]);
     cfg.density = atof(argv[3]);
     cfg.seed = (uint)strtoul(argv[4], 0, 10);
@@ -30,7 +33,14 @@ int main(int argc, char** argv)
     int nPol = MAX(GetNPol(cfg.density, N, (1 << bl) * (1 << bl) * (1 << bl)), 1);
     CSInit(cs, bl, N, nPol, NULL);
     SetTransTable(&cs[0].con, cfg.polModel);
-    CreatePolymers(&cfg, cs);
+    if (argc > 6) {
+        int rc = ReadLatticeFile(cs, argv[6]);
+        if (rc) { fprintf(stderr, "%s: ReadLatticeFile(%s) failed (%d)\n", argv[0], argv[6], rc); return 2; }
+        rc = CheckIntegrity(cs);
+        if (rc) { fprintf(stderr, "%s: %s fails the integrity check (%d)\n", argv[0], argv[6], rc); return 192; }
+    } else {
+        CreatePolymers(&cfg, cs);
+    }
     struct timespec a, b;
     clock_gettime(CLOCK_MONOTONIC, &a);
     DoMCStep(cs, steps);

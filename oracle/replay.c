@@ -210,6 +210,14 @@ static int replay_head(orc_replay* r, const dom* D, int x, int y, int z, uint32_
 
 void orc_replay_set_linear(orc_replay* r, int linear) { r->linear = linear ? 1 : 0; }
 
+void orc_replay_set_state(orc_replay* r, const uint32_t* lat, const uint32_t* rec, uint64_t step)
+{
+    const size_t S = (size_t)r->g.L * r->g.L * r->g.L;
+    memcpy(r->lat, lat, S * sizeof(uint32_t));
+    memcpy(r->rec, rec, 4 * (size_t)r->P * sizeof(uint32_t));
+    r->step = step;
+}
+
 orc_replay* orc_replay_new(const orc_geom* g, int N, int P, uint32_t seed, uint32_t salt)
 {
     tab_init();

@@ -2,7 +2,9 @@
 
 Run in a checkout where the reference sources are available:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]
+
+(--ref defaults to the environment variable ELP_REFERENCE.)
 
 It compiles the reference's efpol from its own sources (oracle/Makefile target
 ``ref``; outputs only under oracle/_ref/), then records
@@ -174,25 +176,71 @@ def make_linear(refdir, tmp):
                 os.path.join(tmp, "lin_stats"))
 
 
-def write_stats(binary, prefix, engine, cases, tmp):
+def write_stats(binary, prefix, engine, cases, tmp, workers=1):
+    from concurrent.futures import ThreadPoolExecutor
+
     for (L, N, tmax, interval, therm, seeds) in cases:
-        per_seed = []
-        for s in seeds:
+        def one(s):
             d = run_efpol(binary, s, L, N, tmax, interval, tmp)
             rg, sl, hist, msd = stats_of_run(d, tmax, interval, L, therm)
-            per_seed.append({"seed": s, "rg2": rg, "sl_frac": sl, "run_hist": hist, "msd": msd})
             shutil.rmtree(os.path.dirname(d))
+            return {"seed": s, "rg2": rg, "sl_frac": sl, "run_hist": hist, "msd": msd}
+
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            per_seed = list(ex.map(one, seeds))
         out = {"engine": engine, "L": L, "N": N, "density": 1.2, "steps": tmax, "interval": interval, "therm": therm,
                "msd_lags_intervals": STAT_LAGS, "per_seed": per_seed}
         with open(os.path.join(HERE, f"{prefix}_stats_L{L}_N{N}.json"), "w") as f:
             json.dump(out, f, indent=1)
 
 
+def make_lowm(refdir, tmp):
+    """The reference's own statistics program on the reference's own
+    trajectory: create_ptl then lowm_modes on efpol's L=16, N=50 dumps
+    (t = 0..100, every 10; the efpol_L16_N50_s3_t*.res.gz fixtures).  Keeps
+    rgyr_time.dat (mean Rg^2 per dump), slrat.dat (stored-length ratio per
+    dump) and cmsdif_raw.dat (centre-of-mass MSD per lag) as
+    lowm_L16_N50_s3.json; oracle/observables.py is checked against them."""
+    d = os.path.join(tmp, "lowm")
+    os.makedirs(d)
+    for t in range(0, 101, 10):
+        with gzip.open(os.path.join(HERE, f"efpol_L16_N50_s3_t{t}.res.gz"), "rb") as f, \
+                open(os.path.join(d, f"t={t}_dev=0.res"), "wb") as g:
+            g.write(f.read())
+    with open(os.path.join(d, "simulation_settings.txt"), "w") as f:
+        f.write("Start_seed = 3\nLength = 50\nPolytype = ring\nDensity = 1.200000\nLatsize = 16\n"
+                "Start_polysize = 50\nDouble_step = 0\nInterval = 10\nExecutable = efpol\n"
+                "Polymodel = sl_equal\nEquilibrated = 1\n")
+    subprocess.run([os.path.join(refdir, "create_ptl"), d], check=True, stdout=subprocess.DEVNULL)
+    subprocess.run([os.path.join(refdir, "lowm_modes"), d], check=True, stdout=subprocess.DEVNULL)
+
+    def table(name):
+        with open(os.path.join(d, name)) as f:
+            return [[float(x) for x in ln.split()] for ln in f if ln.strip()]
+
+    out = {"source": "reference create_ptl + lowm_modes (analysis/), built from source, on efpol_L16_N50_s3 dumps",
+           "rgyr_time": table("rgyr_time.dat"), "slrat": table("slrat.dat"), "cmsdif_raw": table("cmsdif_raw.dat")}
+    with open(os.path.join(HERE, "lowm_L16_N50_s3.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+def make_tiled_stats(efpol, tmp):
+    """An L=64 ensemble, the box the GPU runs in tiles (32^3 or 32x16x16):
+    efpol rounds L to a power of two, so 64 is the largest box it runs in
+    minutes.  Compared with tiled GPU runs in tests/test_gpu_stats.py."""
+    write_stats(efpol, "efpol", "reference efpol_ring (cpupol, sl_equal), built from source",
+                [(64, 100, 10000, 100, 3000, range(601, 617, 2))], tmp, workers=os.cpu_count() or 1)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["all", "ptl", "double", "export", "pov", "linear"], default="all")
+    ap.add_argument("--ref", default=os.environ.get("ELP_REFERENCE"),
+                    help="reference checkout (default: $ELP_REFERENCE)")
+    ap.add_argument("--only", choices=["all", "ptl", "double", "export", "pov", "linear", "tiled", "lowm"],
+                    default="all")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("name the reference checkout with --ref or ELP_REFERENCE")
     subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={args.ref}"], check=True,
                    stdout=subprocess.DEVNULL)
     refdir = os.path.join(REPO, "oracle", "_ref")
@@ -213,6 +261,12 @@ def main():
             return
         if args.only == "linear":
             make_linear(refdir, tmp)
+            return
+        if args.only == "tiled":
+            make_tiled_stats(efpol, tmp)
+            return
+        if args.only == "lowm":
+            make_lowm(refdir, tmp)
             return
         for name, code in MODELS.items():
             raw = os.path.join(tmp, f"tab_{name}.bin")
@@ -237,6 +291,8 @@ def main():
         make_export(refdir, tmp)
         make_pov(refdir, tmp)
         make_linear(refdir, tmp)
+        make_tiled_stats(efpol, tmp)
+        make_lowm(refdir, tmp)
 
         # efpol's seeding drops bit 0 of every Tausworthe word (util/rng.h:13-20,
         # 26-31), so seeds 2k and 2k+1 give the same run: use odd seeds only.

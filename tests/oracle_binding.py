@@ -41,6 +41,7 @@ def lib():
         L.orc_replay_export.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_replay_steps.argtypes = [C.c_void_p, C.c_long]
         L.orc_replay_set_linear.argtypes = [C.c_void_p, C.c_int]
+        L.orc_replay_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64]
         _LIB = L
     return _LIB
 
@@ -126,6 +127,13 @@ class Replay:
 
     def steps(self, n):
         lib().orc_replay_steps(self.h, n)
+
+    def set_state(self, words, records, step):
+        """Continue from a given state (site words, records) at absolute `step`."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        records = np.ascontiguousarray(records, dtype=np.uint32)
+        assert words.shape == (self.L ** 3,) and records.shape == (self.P, 4)
+        lib().orc_replay_set_state(self.h, words.ctypes.data, records.ctypes.data, step)
 
     def _struct(self):
         # orc_replay: geom(6 ints), N, P, seed, salt, uint64 step, lat*, rec*, accepted, attempted
