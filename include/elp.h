@@ -55,8 +55,10 @@ typedef struct elp_job_spec {
     int32_t tile[3];          /* tiled domain edges, 0 = auto */
     int32_t ncol;             /* colour modulus, 0 = auto */
     int32_t device;           /* CUDA device ordinal */
-    int32_t steps_per_launch; /* steps per kernel launch (>=1); tiled domains: a cooperative launch with a
-                                 grid barrier between steps.  Any value gives the same bits. */
+    int32_t steps_per_launch; /* steps per kernel launch (>=1); tiled domains: the launch's tiles of
+                                 consecutive steps run as a dataflow, each tile waiting only for the
+                                 tiles of the previous step that overlap it.  Any value gives the
+                                 same bits. */
     int32_t kernel;           /* 0 auto (specialised when the shape has one), 1 generic */
     int32_t linear;           /* 0 ring polymers (efpol_ring), 1 linear chains (efpol_lin): the last
                                * bond of every chain is the end marker 0xf ('f' in TUV files).
@@ -121,6 +123,14 @@ elp_status elp_sync(elp_ctx* ctx);
  * asynchronously behind the walk, itself queued behind the steps. */
 elp_status elp_fetch_chains(elp_ctx* ctx, int32_t* start, uint8_t* bonds);
 
+/* elp_fetch_chains and elp_check in one pass over the melt (one ring walk,
+ * one site scan): the rings go to start[3*P] / bonds[P*N] and the integrity
+ * code (0 ok, 3, 4: efpol's codes, cpupol/efpol_io.c:158-211) to *code.
+ * With a non-zero code the buffers are unspecified.  The drop-in programs
+ * check every dump this way (the reference checks only before and after the
+ * run, cpupol/efpol.c:68,111).  Blocking. */
+elp_status elp_fetch_checked(elp_ctx* ctx, int32_t* start, uint8_t* bonds, int32_t* code);
+
 /* Write the current state as a TUV file, byte-compatible with the
  * reference's WriteLatticeFile.  Blocking. */
 elp_status elp_write_tuv(elp_ctx* ctx, const char* path);
@@ -172,8 +182,22 @@ elp_status elp_observe(elp_ctx* ctx, double* cms_tuv, double* rg2, double* sl, u
 elp_status elp_get_state(elp_ctx* ctx, uint32_t* words, uint32_t* records);
 elp_status elp_set_state(elp_ctx* ctx, const uint32_t* words, const uint32_t* records, uint64_t step);
 
-/* Moves accepted since creation (counted on the device). */
+/* Moves accepted since creation (counted on the device).  Returns
+ * ELP_ERR_STATE, with the count as it stands, if an earlier launch reported
+ * an error (its steps are incomplete), as elp_sync does. */
 elp_status elp_accepted(elp_ctx* ctx, uint64_t* accepted);
+
+/* Bound of the waits inside tiled launches of several steps.  No counterpart
+ * in the reference, whose launches take one step each (gpupol2/gpupol_cuda.cu:
+ * 129-146).  A tile of step s waits for the tiles of step s - 1 that overlap
+ * it; a wait gives up after `polls` polls (0: the default, about a second)
+ * and the launch then reports ELP_ERR_STATE at the next synchronising call.
+ * The context stays usable: loading a configuration (elp_init_melt, a load
+ * call, elp_set_state) clears the report.  hold_tile >= 0 is a test hook:
+ * that tile (work-item index) never announces its first step of a launch,
+ * so the tiles waiting on it run out of polls -- the failure path is tested
+ * without faulting or hanging the GPU.  -1 announces every tile. */
+elp_status elp_debug_waits(elp_ctx* ctx, uint32_t polls, int32_t hold_tile);
 
 void elp_destroy(elp_ctx* ctx);
 
@@ -236,9 +260,10 @@ const char* elp_last_error(void);
  * one packed arena; melts with the same domain geometry share one kernel
  * launch and a stream, and groups of different shapes run concurrently.
  * Melts run `steps_per_launch` steps per launch: whole-box melts (L <= 32)
- * on chip, tiled melts as one cooperative launch whose CTAs meet at a grid
- * barrier between steps (in a batch of more than one group, tiled groups take
- * one step per launch, so that groups keep overlapping); tiled launches are
+ * on chip, tiled melts as one persistent launch whose tiles of consecutive
+ * steps wait only for the tiles they overlap (in a batch of more than one
+ * group, tiled groups take one step per launch, so that groups keep
+ * overlapping); tiled launches are
  * replayed from a CUDA graph.  A melt gives the same bits in a batch as alone
  * with the same spec, whatever its steps per launch.
  * The reference has no batched engine; its nearest form is one independent

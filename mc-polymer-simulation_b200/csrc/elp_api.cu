@@ -138,6 +138,8 @@ static elp_status upload(elp_ctx* c, const uint32_t* lat, const uint32_t* rec, u
     ELP_CUDA_TRY(cudaMemcpyAsync(c->d_lat, lat, S * 4, cudaMemcpyHostToDevice, c->stream));
     ELP_CUDA_TRY(cudaMemcpyAsync(c->d_rec, rec, (size_t)c->P * ELP_REC_WORDS * 4, cudaMemcpyHostToDevice, c->stream));
     ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, step));
+    // a new configuration replaces whatever an earlier failed launch left
+    ELP_CUDA_TRY(cudaMemsetAsync(error_flags(c), 0, sizeof(uint32_t), c->stream));
     ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->loaded = 1;
     return ELP_OK;
@@ -152,6 +154,7 @@ extern "C" elp_status elp_load_chains(elp_ctx* c, const int32_t* start, const ui
     // whose status read-back is the call's one synchronisation.
     c->loaded = 0;
     ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, step));
+    ELP_CUDA_TRY(cudaMemsetAsync(error_flags(c), 0, sizeof(uint32_t), c->stream));
     elp_status st = elp_build_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, start, bonds, &c->wb, c->stream);
     if (st) return st;
     c->loaded = 1;
@@ -166,6 +169,7 @@ extern "C" elp_status elp_init_melt(elp_ctx* c)
     elp_status st = elp_init_melt_device(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, c->stream);
     if (st) return st;
     ELP_CUDA_TRY(elp_group_set_step(&c->G, 0, 0));
+    ELP_CUDA_TRY(cudaMemsetAsync(error_flags(c), 0, sizeof(uint32_t), c->stream));
     ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->loaded = 1;
     return ELP_OK;
@@ -233,6 +237,23 @@ extern "C" elp_status elp_accepted(elp_ctx* c, uint64_t* acc)
     ELP_CUDA_TRY(cudaMemcpyAsync(&v, c->d_acc, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
     ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
     *acc = v;
+    return elp_device_errors(error_flags(c), c->stream);
+}
+
+extern "C" elp_status elp_debug_waits(elp_ctx* c, uint32_t polls, int32_t hold_tile)
+{
+    if (!c) return elp_fail(ELP_ERR_ARG, "null context");
+    if (hold_tile < -1 || (c->G.nitems > 0 && hold_tile >= c->G.nitems))
+        return elp_fail(ELP_ERR_ARG, "tile %d not in 0..%d", hold_tile, c->G.nitems - 1);
+    ELP_CUDA_TRY(cudaSetDevice(c->device));
+    ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->G.wait_polls = polls;
+    c->G.hold_item1 = hold_tile + 1;
+    if (c->G.graph) {
+        // captured launches carry the old bound: capture again on the next run
+        cudaGraphExecDestroy(c->G.graph);
+        c->G.graph = nullptr;
+    }
     return ELP_OK;
 }
 
@@ -245,6 +266,17 @@ extern "C" elp_status elp_fetch_chains(elp_ctx* c, int32_t* start, uint8_t* bond
     // between); the launches' error flags are read after it and take
     // precedence over the walk's status
     elp_status st = elp_fetch_rings(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, start, bonds, c->stream);
+    elp_status fl = elp_device_errors(error_flags(c), c->stream);
+    return fl ? fl : st;
+}
+
+extern "C" elp_status elp_fetch_checked(elp_ctx* c, int32_t* start, uint8_t* bonds, int32_t* code)
+{
+    if (!c || !start || !bonds || !code) return elp_fail(ELP_ERR_ARG, "null argument");
+    if (!c->loaded) return elp_fail(ELP_ERR_STATE, "no configuration loaded");
+    ELP_CUDA_TRY(cudaSetDevice(c->device));
+    elp_status st = elp_fetch_checked_melt(c->d_lat, c->d_rec, c->g.L, c->N, c->P, c->linear, &c->wb, start, bonds,
+                                           code, c->stream);
     elp_status fl = elp_device_errors(error_flags(c), c->stream);
     return fl ? fl : st;
 }

@@ -121,8 +121,8 @@ elp_status elp_device_errors(const uint32_t* d_flags, cudaStream_t s)
         return elp_fail(ELP_ERR_STATE, "a domain held more monomer-0 runs than its label table; steps after the "
                                        "overflow are incomplete (use the generic kernel for this melt)");
     if (flags & 4u)
-        return elp_fail(ELP_ERR_STATE, "a tiled launch of several steps gave up waiting at its grid barrier; steps "
-                                       "after it are incomplete");
+        return elp_fail(ELP_ERR_STATE, "a tile gave up waiting for the tiles of the previous step; steps after it "
+                                       "are incomplete");
     return ELP_OK;
 }
 
@@ -130,6 +130,7 @@ void elp_walk_bufs_free(elp_walk_bufs* b)
 {
     cudaFree(b->d_start); cudaFree(b->d_bonds); cudaFree(b->d_status); cudaFree(b->d_visit); cudaFree(b->d_cnt);
     cudaFree(b->d_obs);
+    cudaFreeHost(b->h_status); cudaFreeHost(b->h_cnt);
     *b = elp_walk_bufs();
 }
 
@@ -179,6 +180,43 @@ elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int 
     for (int p = 0; p < P; p++)
         if (status[(size_t)p])
             return elp_fail(ELP_ERR_INTEGRITY, "ring %d cannot be walked (code %d)", p, status[(size_t)p]);
+    return ELP_OK;
+}
+
+elp_status elp_fetch_checked_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear,
+                                  elp_walk_bufs* b, int32_t* start, uint8_t* bonds, int32_t* code, cudaStream_t s)
+{
+    const size_t S = (size_t)L * L * L;
+    elp_status st = elp_walk_bufs_reserve(b, P, N, S);
+    if (st) return st;
+    if ((size_t)P > b->cap_h_rings) {
+        cudaFreeHost(b->h_status);
+        b->h_status = nullptr;
+        b->cap_h_rings = 0;
+        ELP_CUDA_TRY(cudaMallocHost((void**)&b->h_status, (size_t)P * sizeof(int32_t)));
+        b->cap_h_rings = (size_t)P;
+    }
+    if (!b->h_cnt) ELP_CUDA_TRY(cudaMallocHost((void**)&b->h_cnt, 8 * sizeof(unsigned long long)));
+    ELP_CUDA_TRY(cudaMemsetAsync(b->d_visit, 0, S * sizeof(uint32_t), s));
+    ELP_CUDA_TRY(cudaMemsetAsync(b->d_cnt, 0, 8 * sizeof(unsigned long long), s));
+    WalkArgs w;
+    memset(&w, 0, sizeof(w));
+    w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P; w.linear = linear;
+    w.start = b->d_start; w.bonds = b->d_bonds; w.status = b->d_status; w.visit = b->d_visit; w.counters = b->d_cnt;
+    ELP_CUDA_TRY(elp_launch_walk(&w, s));
+    ELP_CUDA_TRY(elp_launch_scan(&w, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(start, b->d_start, (size_t)P * 3 * 4, cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(bonds, b->d_bonds, (size_t)P * N, cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(b->h_status, b->d_status, (size_t)P * 4, cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(b->h_cnt, b->d_cnt, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaStreamSynchronize(s));
+    int rc = 0;
+    for (int p = 0; p < P && !rc; p++)
+        if (b->h_status[p]) rc = 4;
+    const unsigned long long* cnt = b->h_cnt;
+    if (!rc && cnt[4]) rc = 3;
+    if (!rc && (cnt[0] != cnt[1] || cnt[2] != (unsigned long long)N * P || cnt[3])) rc = 4;
+    *code = rc;
     return ELP_OK;
 }
 

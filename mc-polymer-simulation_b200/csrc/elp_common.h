@@ -34,7 +34,9 @@ struct elp_walk_bufs {
     uint32_t* d_visit = nullptr;
     unsigned long long* d_cnt = nullptr;
     unsigned long long* d_obs = nullptr;   // observables: [P][6] ring sums + histogram
-    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0, cap_obs = 0;
+    int32_t* h_status = nullptr;           // pinned host copies of the ring statuses and counters
+    unsigned long long* h_cnt = nullptr;
+    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0, cap_obs = 0, cap_h_rings = 0;
     size_t bytes = 0;
 };
 void elp_walk_bufs_free(elp_walk_bufs* b);
@@ -55,6 +57,12 @@ elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int 
 // Observables of one melt (elp_observe); any output may be null.
 elp_status elp_observe_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                             double* cms_tuv, double* rg2, double* sl, uint64_t* run_hist, int nbins, cudaStream_t s);
+// Rings of one melt into host buffers (pinned: the copies run behind the
+// walk) together with its integrity code (0, 3 or 4), from one walk and one
+// site scan.  A ring that cannot be walked gives code 4 with ELP_OK: the
+// buffers are then unspecified.
+elp_status elp_fetch_checked_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear,
+                                  elp_walk_bufs* b, int32_t* start, uint8_t* bonds, int32_t* code, cudaStream_t s);
 // Integrity check of one melt (code 0, 3 or 4 as CheckIntegrity).
 elp_status elp_check_melt(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                           int32_t* code, cudaStream_t s);

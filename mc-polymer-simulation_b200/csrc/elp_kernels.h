@@ -9,7 +9,7 @@ struct SweepArgs {
     const uint32_t* table;         // 1024 words = 4096 bytes dst1|dst2<<4
     unsigned long long* accepted;  // optional accepted-move counter
     uint32_t* error;               // device error flags (bit 0: label slot table overflow,
-                                   // bit 2: grid barrier wait gave up)
+                                   // bit 2: a dependency wait gave up)
     int nchains;                   // rings in the melt
     int L, periodic, tx, ty, tz, ncol;
     int sx, sxy, ox, words, groups;
@@ -50,8 +50,16 @@ struct BatchLaunch {
     uint32_t step_base;            // added to every job's step0 ...
     const uint32_t* step_dev;      // ... and, if set, this device counter (graph replays)
     const uint32_t* table;         // 4096-byte transition table
-    uint32_t* error;               // device error flags
-    uint32_t* grid_bar;            // tiled domains, nsteps > 1: {arrivals, exits}, zero between launches
+    uint32_t* error;               // device error flags (bit 0: label slot table overflow,
+                                   // bit 2: a tile's wait for the previous step gave up)
+    // tiled domains: the launch's work items are (step, item) pairs taken in
+    // step order from a ticket counter; a tile waits for the tiles of the
+    // previous step that overlap it on their completion flags
+    uint32_t* flow;                // {ticket, exits}, zero between launches
+    uint32_t* done;                // [nitems] last step (launch-relative, + 1) of each item; zero between launches
+    int njobs;                     // melts in the job table; item index = domain * njobs + melt
+    uint32_t wait_polls;           // polls before a dependency wait gives up (0: about a second)
+    int hold_item1;                // test hook: item + 1 whose first step is never announced (0: none)
 };
 
 #include "elp_internal.h"

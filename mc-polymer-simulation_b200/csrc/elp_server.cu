@@ -9,8 +9,13 @@
 // small latency-bound melt never holds up the GPU.  Lattices stay resident
 // between dumps.  At a dump the job's state is copied device-to-device on
 // the group's stream at the end of the tick; I/O threads, each with its own
-// stream and scratch, rebuild the rings from the copy, check the final state
-// and format the TUV text while the group keeps computing.  A job follows
+// stream, scratch and pinned host buffers, rebuild the rings from the copy,
+// check the melt's invariants (every dump, as CheckIntegrity), and format
+// and write the TUV text while the group keeps computing.  A dump that fails
+// its check or its write ends the job with that status at the group's next
+// tick.  Queued jobs are admitted in order; a job that does not fit the
+// budget lets smaller ones behind it pass, until it has been passed
+// ADMIT_PASSES times: then it holds its place and the memory it waits for.  A job follows
 // the same trajectory alone, in any mix, or through the single-melt API: its
 // kernel, counters and geometry depend only on its spec.
 //
@@ -68,13 +73,19 @@ struct SJob {
     int integrity = -1;
     uint64_t checksum = 0;
     std::string error;
+    int passed = 0;                       // queued: times a job behind it was admitted first
+    std::atomic<int> abort{0};            // set by an I/O thread: a dump failed (status code)
+    std::atomic<int> pending{0};          // snapshots queued or in work
+    std::atomic<bool> final_seen{false};  // the last snapshot (or the abort marker) is done
 };
 
-// A snapshot on its way to the host.
+// A snapshot on its way to the host.  An abort marker (no state) ends a job
+// whose dump failed.
 struct Snap {
     SJob* job = nullptr;
     int64_t step = 0;
     bool final = false;
+    bool abort = false;
     uint32_t* d_lat = nullptr;            // copy of the job's state at `step`
     uint32_t* d_rec = nullptr;
     cudaEvent_t ready = nullptr;          // recorded after the copy on the group's stream
@@ -133,16 +144,54 @@ struct elp_server {
 
 static void fail_job(elp_server* s, SJob* j, elp_status st, const char* msg);
 
+// Publish a finished job once its last snapshot and every earlier one are
+// done (several I/O threads may hold snapshots of one job).
+static void snapshot_done(elp_server* s, SJob* j, bool last)
+{
+    if (last) j->final_seen = true;
+    if (--j->pending == 0 && j->final_seen.load()) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        j->t_done = s->now();
+        s->finished.push_back(j);
+        s->completed++;
+        s->cv_done.notify_all();
+    }
+}
+
+// A dump failed: the first failure decides the job's status.
+static void dump_failed(elp_server* s, SJob* j, elp_status st, const std::string& msg)
+{
+    int expect = 0;
+    if (j->abort.compare_exchange_strong(expect, (int)st)) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        j->status = st;
+        j->error = msg;
+    }
+}
+
+// Write a TUV file; ELP_ERR_IO on any failure (open, short write, close).
+static elp_status write_text(const char* path, const std::string& text, size_t len)
+{
+    FILE* f = fopen(path, "wb");
+    if (!f) return elp_fail(ELP_ERR_IO, "cannot open %s for writing", path);
+    const size_t n = fwrite(text.data(), 1, len, f);
+    const int c = fclose(f);
+    if (n != len || c != 0) return elp_fail(ELP_ERR_IO, "writing %s failed (%zu of %zu bytes)", path, n, len);
+    return ELP_OK;
+}
+
 // One I/O thread: rebuilds the rings of snapshots on its own stream and
-// scratch, checks the final state of a job, writes its TUV text.
+// scratch into pinned host buffers, checks the melt's invariants, writes its
+// TUV text.
 static void io_worker(elp_server* s)
 {
     cudaSetDevice(s->o.device);
     cudaStream_t st = nullptr;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     elp_walk_bufs wb;
-    std::vector<int32_t> start;
-    std::vector<uint8_t> bonds;
+    int32_t* h_start = nullptr;   // pinned, grown as jobs need
+    uint8_t* h_bonds = nullptr;
+    size_t cap_start = 0, cap_bonds = 0;
     for (;;) {
         Snap sn;
         {
@@ -153,53 +202,77 @@ static void io_worker(elp_server* s)
             s->io_q.pop_front();
         }
         SJob* j = sn.job;
+        if (sn.abort) {
+            snapshot_done(s, j, true);
+            s->io_busy--;
+            continue;
+        }
         const int L = j->g.L, N = j->spec.N, P = j->P;
-        start.resize((size_t)P * 3);
-        bonds.resize((size_t)P * N);
+        elp_status rc = ELP_OK;
+        if ((size_t)P * 3 > cap_start) {
+            cudaFreeHost(h_start);
+            h_start = nullptr;
+            cap_start = 0;
+            if (cudaMallocHost((void**)&h_start, (size_t)P * 3 * sizeof(int32_t)) == cudaSuccess)
+                cap_start = (size_t)P * 3;
+            else
+                rc = elp_fail(ELP_ERR_NOMEM, "pinned host buffer of %d rings", P);
+        }
+        if (rc == ELP_OK && (size_t)P * N > cap_bonds) {
+            cudaFreeHost(h_bonds);
+            h_bonds = nullptr;
+            cap_bonds = 0;
+            if (cudaMallocHost((void**)&h_bonds, (size_t)P * N) == cudaSuccess)
+                cap_bonds = (size_t)P * N;
+            else
+                rc = elp_fail(ELP_ERR_NOMEM, "pinned host buffer of %d x %d bonds", P, N);
+        }
         cudaStreamWaitEvent(st, sn.ready, 0);
         const int lin = j->spec.linear ? 1 : 0;
-        elp_status rc = elp_fetch_rings(sn.d_lat, sn.d_rec, L, N, P, lin, &wb, start.data(), bonds.data(), st);
-        if (sn.final && rc == ELP_OK) {
-            int32_t code = -1;
-            if (elp_check_melt(sn.d_lat, sn.d_rec, L, N, P, lin, &wb, &code, st) == ELP_OK) j->integrity = code;
-        }
+        int32_t code = -1;
+        if (rc == ELP_OK)
+            rc = elp_fetch_checked_melt(sn.d_lat, sn.d_rec, L, N, P, lin, &wb, h_start, h_bonds, &code, st);
         std::string err = rc == ELP_OK ? std::string() : std::string(elp_last_error());
         cudaFreeAsync(sn.d_lat, st);
         cudaFreeAsync(sn.d_rec, st);
         cudaStreamSynchronize(st);
         cudaEventDestroy(sn.ready);
-        if (rc != ELP_OK) {
-            if (sn.final) fail_job(s, j, rc, err.c_str());
-            s->io_busy--;
-            continue;
-        }
-        if (!j->dir.empty()) {
-            size_t len = 0;
-            elp_format_tuv(L, N, P, start.data(), bonds.data(), nullptr, 0, &len);
-            std::string text(len + 1, '\0');
-            elp_format_tuv(L, N, P, start.data(), bonds.data(), &text[0], len + 1, &len);
-            char path[4096];
-            snprintf(path, sizeof(path), "%s/t=%lld_dev=0.res", j->dir.c_str(), (long long)sn.step);
-            FILE* f = fopen(path, "wb");
-            if (f) {
-                fwrite(text.data(), 1, len, f);
-                fclose(f);
+        if (rc == ELP_OK) {
+            if (sn.final || code != 0) {
+                std::lock_guard<std::mutex> lk(s->mu);
+                j->integrity = code;
+            }
+            if (code != 0) {
+                rc = ELP_ERR_INTEGRITY;
+                char m[160];
+                snprintf(m, sizeof(m), "integrity check failed at step %lld (code %d)", (long long)sn.step, code);
+                err = m;
             }
         }
-        if (sn.final) {
-            uint64_t h = 0xcbf29ce484222325ULL;
-            h = fnv1a(h, start.data(), start.size() * sizeof(int32_t));
-            h = fnv1a(h, bonds.data(), bonds.size());
-            j->checksum = h;
-            std::lock_guard<std::mutex> lk(s->mu);
-            j->t_done = s->now();
-            s->finished.push_back(j);
-            s->completed++;
-            s->cv_done.notify_all();
+        if (rc == ELP_OK && !j->dir.empty()) {
+            size_t len = 0;
+            elp_format_tuv(L, N, P, h_start, h_bonds, nullptr, 0, &len);
+            std::string text(len + 1, '\0');
+            elp_format_tuv(L, N, P, h_start, h_bonds, &text[0], len + 1, &len);
+            char path[4096];
+            snprintf(path, sizeof(path), "%s/t=%lld_dev=0.res", j->dir.c_str(), (long long)sn.step);
+            rc = write_text(path, text, len);
+            if (rc != ELP_OK) err = elp_last_error();
         }
+        if (rc != ELP_OK) {
+            dump_failed(s, j, rc, err);
+        } else if (sn.final) {
+            uint64_t h = 0xcbf29ce484222325ULL;
+            h = fnv1a(h, h_start, (size_t)P * 3 * sizeof(int32_t));
+            h = fnv1a(h, h_bonds, (size_t)P * N);
+            j->checksum = h;
+        }
+        snapshot_done(s, j, sn.final);
         s->io_busy--;
     }
     elp_walk_bufs_free(&wb);
+    cudaFreeHost(h_start);
+    cudaFreeHost(h_bonds);
     cudaStreamDestroy(st);
 }
 
@@ -218,8 +291,8 @@ static SGroup* group_for(elp_server* s, SJob* j)
         return nullptr;
     // membership changes every few ticks: a captured graph would be rebuilt
     // about as often as it is replayed, so tiled groups launch directly, one
-    // step per launch (a launch of several tiled steps is cooperative and
-    // holds every SM it uses until its last step, stalling the other groups)
+    // step per launch (a launch of several tiled steps keeps its persistent
+    // CTAs on every SM it uses until its last step, stalling the other groups)
     gp->G.use_graph = 0;
     if (!j->g.periodic) gp->G.spl = 1;
     s->groups.push_back(std::move(gp));
@@ -238,23 +311,44 @@ static void fail_job(elp_server* s, SJob* j, elp_status st, const char* msg)
 }
 
 // Admit queued jobs that fit the budget; returns false on a fatal CUDA error.
+// Jobs are taken in queue order.  A job that does not fit the memory left
+// lets the jobs behind it pass (no head-of-line blocking) until it has been
+// passed ADMIT_PASSES times; from then on it sets aside the memory it needs,
+// and a job behind it is admitted only if it fits next to everything set
+// aside ahead of it, so a large job is never starved by a stream of small
+// ones.  The scan looks at most ADMIT_SCAN queued jobs.
+static constexpr int ADMIT_SCAN = 256;
+static constexpr int ADMIT_PASSES = 64;
 static bool admit(elp_server* s)
 {
-    for (;;) {
-        SJob* j = nullptr;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            if (s->queue.empty()) return true;
-            SJob* c = s->queue.front();
-            if (s->resident.size() >= (size_t)s->o.max_jobs) return true;
-            if (s->bytes_in_use + c->bytes > s->o.hbm_budget && !s->resident.empty()) return true;
-            s->queue.pop_front();
-            j = c;
+    std::vector<SJob*> take, refuse;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        size_t in_use = s->bytes_in_use, reserved = 0;
+        const size_t budget = s->o.hbm_budget;
+        std::vector<SJob*> waiting;           // jobs ahead that did not fit
+        int scanned = 0;
+        for (auto it = s->queue.begin(); it != s->queue.end() && scanned < ADMIT_SCAN; scanned++) {
+            if (s->resident.size() + take.size() >= (size_t)s->o.max_jobs) break;
+            SJob* c = *it;
+            if (c->bytes > budget) {
+                refuse.push_back(c);
+                it = s->queue.erase(it);
+            } else if (in_use + reserved + c->bytes <= budget) {
+                take.push_back(c);
+                in_use += c->bytes;
+                for (SJob* w : waiting) w->passed++;
+                it = s->queue.erase(it);
+            } else {
+                waiting.push_back(c);
+                if (c->passed >= ADMIT_PASSES) reserved += c->bytes;
+                if (in_use + reserved >= budget) break;   // nothing behind it can pass
+                ++it;
+            }
         }
-        if (j->bytes > s->o.hbm_budget) {
-            fail_job(s, j, ELP_ERR_BUSY, "job needs more device memory than the server budget");
-            continue;
-        }
+    }
+    for (SJob* j : refuse) fail_job(s, j, ELP_ERR_BUSY, "job needs more device memory than the server budget");
+    for (SJob* j : take) {
         SGroup* gp = group_for(s, j);
         if (!gp) {
             fail_job(s, j, ELP_ERR_CUDA, "cannot create a group for the job");
@@ -278,14 +372,12 @@ static bool admit(elp_server* s)
             if (s->groups[g].get() == gp) j->group = (int)g;
         gp->members.push_back(j);
         gp->dirty = true;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->bytes_in_use += j->bytes;
-        }
         j->t_start = s->now();
         std::lock_guard<std::mutex> lk(s->mu);
+        s->bytes_in_use += j->bytes;
         s->resident.push_back(j);
     }
+    return true;
 }
 
 static bool rebuild(elp_server* s, SGroup* gp)
@@ -335,6 +427,24 @@ static bool complete_tick(elp_server* s, SGroup* gp, size_t gi)
             std::lock_guard<std::mutex> lk(s->mu);
             s->moves_done += (double)Q * j->spec.N * j->P;
         }
+        if (j->abort.load()) {
+            // an earlier dump failed: end the job (its status is set); the
+            // marker reaches the I/O threads after its queued snapshots
+            Snap sn;
+            sn.job = j;
+            sn.step = j->done_steps;
+            sn.final = true;
+            sn.abort = true;
+            j->pending++;
+            s->io_busy++;
+            {
+                std::lock_guard<std::mutex> lk(s->io_mu);
+                s->io_q.push_back(sn);
+            }
+            s->io_cv.notify_one();
+            done.push_back(j);
+            continue;
+        }
         const bool fin = j->done_steps >= j->nsteps;
         const bool dump = j->dump_interval > 0 && j->done_steps % j->dump_interval == 0;
         if (dump || fin) {
@@ -354,6 +464,7 @@ static bool complete_tick(elp_server* s, SGroup* gp, size_t gi)
             cudaMemcpyAsync(sn.d_rec, j->rec, (size_t)j->P * ELP_REC_WORDS * 4, cudaMemcpyDeviceToDevice, gp->s);
             cudaEventRecord(sn.ready, gp->s);
             if (dump) j->dumps++;
+            j->pending++;
             s->io_busy++;
             {
                 std::lock_guard<std::mutex> lk(s->io_mu);
@@ -449,6 +560,10 @@ static void scheduler(elp_server* s)
     for (auto& gp : s->groups)
         if (gp->busy) cudaEventSynchronize(gp->ev);
     if (s->fatal) {
+        // the I/O threads may still hold snapshots of resident jobs: let them
+        // finish (bounded) before the jobs are handed back
+        for (int i = 0; i < 60000 && s->io_busy.load() > 0; i++)
+            std::this_thread::sleep_for(std::chrono::milliseconds(1));
         std::lock_guard<std::mutex> lk(s->mu);
         for (SJob* j : s->resident) {
             j->status = s->fatal;
@@ -638,12 +753,23 @@ extern "C" void elp_server_destroy(elp_server* s)
         std::this_thread::sleep_for(std::chrono::milliseconds(5));
     }
     if (s->sched.joinable()) s->sched.join();
-    while (s->io_busy.load() > 0) std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    // the last snapshots: each takes a walk, a check and a file write; give
+    // them a generous bound.  If the I/O threads do not finish in time they
+    // are left running with the server's host state (leaked, not freed under
+    // them) and only the call returns.
+    bool io_done = false;
+    for (int i = 0; i < 300000 && !(io_done = s->io_busy.load() == 0); i++)
+        std::this_thread::sleep_for(std::chrono::milliseconds(1));
     {
         std::lock_guard<std::mutex> lk(s->io_mu);
         s->io_stop = true;
     }
     s->io_cv.notify_all();
+    if (!io_done) {
+        elp_fail(ELP_ERR_BUSY, "server I/O threads still busy after 300 s; server state leaked");
+        for (auto& t : s->io_threads) t.detach();
+        return;
+    }
     for (auto& t : s->io_threads) t.join();
     cudaSetDevice(s->o.device);
     for (auto& gp : s->groups) {

@@ -3,14 +3,22 @@
 // Same schedule and results as the generic sweep_kernel (elp_sweep.cu); what
 // changes is how the work is fed to the SM:
 //   * tile edges and shared-memory strides are compile-time constants;
-//   * the four anchors a thread owns in a substep are processed stage by
-//     stage (all first loads, then all second loads, ...), so the dependent
-//     shared-memory loads of four independent moves overlap;
+//   * a ring substep runs in two phases.  Phase 1 reads, for every anchor,
+//     the words the move depends on (anchor, next run, target) and decides
+//     acceptance without storing anything.  The warp's accepted moves are
+//     queued in shared memory (one word each), and phase 2 commits them with
+//     the warp's lanes taking queue entries in order: the new words, the
+//     bookkeeping of monomer 0 and the stores run once per accepted move
+//     instead of once per anchor;
 //   * monomer 0's runs are handled inline: while a tile is on chip each
 //     labelled word carries its run length (bits 16-31) and a slot number
-//     (bits 5-15) into a small shared-memory table {chain, offset, site};
+//     (bits 5-15) into a small shared-memory table {chain, offset | site};
 //     the chain records in global memory are read when the tile is loaded and
-//     written back when it is stored, so no move waits on global memory;
+//     written back when it is stored, so no move waits on global memory.  A
+//     ring tile that holds more monomer-0 runs than the table (short rings
+//     crowded together, as CreatePolymers leaves them) runs its substeps with
+//     the general move of elp_device.cuh instead, which keeps that
+//     bookkeeping in the chain records: slower, the same bits;
 //   * a tile's rows are fetched in 16-byte cp.async granules.  The origin
 //     shift makes a row start anywhere, so each row fetch takes the 16-byte
 //     aligned span around the row (TX + 4 words) and the tile sits
@@ -19,8 +27,11 @@
 //     the ragged ends).  Rows are 16-byte aligned in shared memory, and the
 //     threads of a warp take anchors from an 8 x 4 block of rows so that
 //     their first loads hit 32 different banks;
-//   * the grid is persistent over the tiles, and a launch of several steps
-//     over a tiled box is cooperative, with a grid barrier between steps.
+//   * tiled melts are scheduled as a dataflow over (step, tile) items: CTAs
+//     take items from a ticket counter in step order, and a tile of step s
+//     waits only for the (at most 8) tiles of step s - 1 that overlap it, on
+//     per-tile completion flags.  No CTA waits for the whole grid, and the
+//     tiles of consecutive steps overlap in time.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -49,37 +60,13 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p)
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-constexpr int GRID_POLLS = 1 << 24;
-
-// Barrier over all CTAs of a cooperative launch: each CTA adds one to
-// bar[0] and waits (bounded) until it reaches `target`.  The CTA's stores
-// before it are visible to every CTA's loads after it (tiles are fetched
-// with cp.async.cg and records with ld.global.cg, both through L2).
-// Returns false, in every thread of the CTA, when the wait gave up.
-__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t target)
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v)
 {
-    bool ok = true;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(bar, 1u);
-        for (int n = 0; ld_acquire_gpu(bar) < target; n++) {
-            if (n >= GRID_POLLS) { ok = false; break; }
-            __nanosleep(64);
-        }
-    }
-    return __syncthreads_or(!ok) == 0;
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
-// Last act of every CTA of a cooperative launch: the last one to leave
-// zeroes the barrier counts for the next launch on the stream.
-__device__ __forceinline__ void grid_exit(uint32_t* bar)
-{
-    __syncthreads();
-    if (threadIdx.x == 0 && atomicAdd(bar + 1, 1u) == gridDim.x - 1) {
-        atomicExch(bar, 0u);
-        atomicExch(bar + 1, 0u);
-    }
-}
+// Polls of a dependency flag before a wait gives up (about a second with the
+// back-off below); a launch can ask for fewer (BatchLaunch.wait_polls).
+constexpr uint32_t WAIT_POLLS = 1u << 24;
 
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int MINB>
 struct Shape {
@@ -97,18 +84,23 @@ struct Shape {
     static constexpr int SITES = TX * TY * TZ;
     // threads of a warp take anchors from an 8 x 4 block of (y, z) rows
     static constexpr bool PERM = !PER && TY % 8 == 0 && TZ % 4 == 0 && AT % R == 0;
+    // neighbour offsets: 27 boundary classes of a periodic box, one class in a tile
+    static constexpr int NOFF = PER ? 27 * 16 : 16;
     // shared-memory word offsets: lattice, transition table (4096 bytes),
-    // neighbour offsets (27 x 16), colours, slot tables, slot count, and the
-    // Philox words when threads own < 4 anchors
+    // neighbour offsets (bytes, and for tiles in words too), colours, slot
+    // tables, slot count, ticket, head-move rows, per-warp commit queues
+    // (one word per anchor), and the Philox words when threads own < 4 anchors
     static constexpr int TABW = WORDS;
     static constexpr int OFFW = TABW + 1024;
-    static constexpr int COLW = OFFW + 27 * 16;
+    static constexpr int WOFFW = OFFW + NOFF;
+    static constexpr int COLW = WOFFW + (PER ? 0 : 16);
     static constexpr int SCHW = COLW + 64;
-    static constexpr int SOFW = SCHW + CAP;
-    static constexpr int SSIW = SOFW + CAP;
-    static constexpr int NSLW = SSIW + CAP;
-    static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
-    static constexpr int RNDW = (HTABW + 64 + 4) & ~3;
+    static constexpr int SSOW = SCHW + CAP;   // {offset of monomer 0 in its run (bits 0-15), site word (16-31)}
+    static constexpr int NSLW = SSOW + CAP;
+    static constexpr int TKW = NSLW + 1;
+    static constexpr int HTABW = TKW + 1;     // table rows (0xf, x): moves of a linear chain's monomer 0
+    static constexpr int QW = (HTABW + 64 + 3) & ~3;
+    static constexpr int RNDW = (QW + A + 3) & ~3;
     static constexpr int NG = 2 * NC / 4;     // substep groups per step
     static constexpr size_t bytes_with(int groups) { return (size_t)(RNDW + (K < 4 ? groups * G * 4 : 0)) * 4; }
     // Philox words of threads that own < 4 anchors: in tiled domains, where
@@ -120,6 +112,8 @@ struct Shape {
     static constexpr size_t BYTES = (size_t)TOTW * 4;
     static_assert(PER || (SX % 4 == 0 && SXY % 4 == 0 && SX >= SPAN + 1 && SXY >= SX * (TY + 2)),
                   "tiled rows: 16-byte aligned, room for the span and the halo word before it");
+    static_assert(WORDS < 65536, "slot sites are 16-bit word indices");
+    static_assert(BYTES <= 232448, "dynamic shared memory of one CTA");
 };
 
 constexpr uint32_t LMASK = 0xFFF0u;  // label bit + slot number
@@ -133,21 +127,20 @@ constexpr uint32_t HWALL = ELP_CUNIT | 3u;
 extern __shared__ __align__(16) uint32_t g_smem[];
 
 // A labelled word (global form: chain id in bits 5-31) entering shared
-// memory: claim a slot for the chain, keep {chain, offset, site} in the slot
-// table and put the slot number and the run length into the word.  Past the
-// table's capacity the word is left as it is (the overflow is reported
-// before the first substep).
+// memory: claim a slot for the chain, keep {chain, offset | site} in the
+// slot table and put the slot number and the run length into the word.  Past
+// the table's capacity the word is left as it is (the tile then runs the
+// general move).
 template <int CAP>
 __device__ __forceinline__ uint32_t take_slot(uint32_t wv, int idx, const uint32_t* rec, uint32_t* nslots,
-                                              uint32_t* slot_chain, uint32_t* slot_off, int* slot_site)
+                                              uint32_t* slot_chain, uint32_t* slot_so)
 {
     const uint32_t slot = atomicAdd(nslots, 1u);
     if (slot >= (uint32_t)CAP) return wv;
     const uint32_t chain = wv >> 5;
     const uint4 rr = __ldcg(reinterpret_cast<const uint4*>(rec + ELP_REC_WORDS * (size_t)chain));
     slot_chain[slot] = chain;
-    slot_off[slot] = rr.z;
-    slot_site[slot] = idx;
+    slot_so[slot] = rr.z | ((uint32_t)idx << 16);
     return (wv & 15) | ELP_LBIT | (slot << 5) | (rr.y << ELP_CSHIFT);
 }
 
@@ -155,15 +148,148 @@ __device__ __forceinline__ uint32_t take_slot(uint32_t wv, int idx, const uint32
 // load or store needs no index scaling).
 __device__ __forceinline__ uint32_t& SW(int b) { return *reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(g_smem) + b); }
 
-// The K anchors of one thread, one substep.  Returns accepted moves.
-// Anchor q takes its random byte at bit offset bsh[q] of the Philox word w.
-// Byte offsets: anchors base4 + 4 xr, colour c4 = 4 c, neighbour offsets at
-// OFFW words; transition table (bytes) at TABW words.
-template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW, bool LIN>
-__device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, const int (&base4)[K], const int (&rot4)[K],
-                                        const int (&clsyz)[K], const int (&xj4)[K], const int (&bsh)[K],
-                                        const int (&an)[K], int c4, uint32_t w, int L, bool lin, uint32_t t, int d,
-                                        int k, uint2 key)
+// Monomer 0 sits in one of the runs a move touches (src: 0 the anchor's run,
+// 1 the next run, 2 the target run): move its slot's site and offset along.
+// Updates the new word (nP, nB or nY) that ends up holding monomer 0.
+__device__ __forceinline__ void follow_label(uint32_t* slot_so, int p, int pB, int pY, uint32_t wP, uint32_t wB,
+                                             uint32_t wY, uint32_t s, uint32_t d1, uint32_t& nP, uint32_t& nB,
+                                             uint32_t& nY)
+{
+    const int src = (wP & ELP_LBIT) ? 0 : ((s && (wB & ELP_LBIT)) ? 1 : 2);
+    const uint32_t lw = src == 0 ? wP : (src == 1 ? wB : wY);
+    const uint32_t slot = (lw >> 5) & 0x7FFu;
+    const uint32_t off0 = slot_so[slot] & 0xFFFFu;
+    uint32_t noff;
+    int nl;
+    if (src == 0) {
+        nl = 0; noff = off0;
+        if (s == 0 && off0 == (wP >> ELP_CSHIFT) - 1) { nl = 2; noff = 0; }
+    } else if (src == 1) {
+        if (wB >= 2u * ELP_CUNIT && off0 > 0) { nl = 1; noff = off0 - 1; }
+        else { nl = d1 ? 2 : 0; noff = d1 ? 0 : (nP >> ELP_CSHIFT) - 1; }
+    } else {
+        nl = 2; noff = off0 + 1;
+    }
+    const uint32_t lb = lw & LMASK;
+    if (src == 0) nP &= ~LMASK; else if (src == 1) nB &= ~LMASK; else nY &= ~LMASK;
+    if (nl == 0) nP |= lb; else if (nl == 1) nB |= lb; else nY |= lb;
+    slot_so[slot] = noff | ((uint32_t)((nl == 0 ? p : (nl == 1 ? pB : pY)) >> 2) << 16);
+}
+
+// Phase 2 of a ring substep: commit one accepted move from its queue word
+// (bits 0-17 anchor byte offset, 18-25 table entry dst1 | dst2 << 4, 26 slot,
+// 27-31 boundary class of a periodic box).  The words are read again: the
+// footprints of a substep's anchors are disjoint, so they still hold what
+// phase 1 read.  Store order B, Y, P: when dst1 == 0 the target is P itself
+// and P's store must come last.
+template <bool PER, int OFFW>
+__device__ __forceinline__ void commit_ring(uint32_t* slot_so, uint32_t qe)
+{
+    const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
+    const int p = (int)(qe & 0x3FFFFu);
+    const uint32_t d1 = (qe >> 18) & 15u, d2 = (qe >> 22) & 15u, s = (qe >> 26) & 1u;
+    const int ob = PER ? 16 * (int)(qe >> 27) : 0;
+    const uint32_t wP = SW(p);
+    const int pB = p + offs[ob + (wP & 15)];
+    const int pY = p + offs[ob + d1];
+    const uint32_t wB = SW(pB), wY = SW(pY);
+    uint32_t nP = wP & ~15u;
+    nP = (s == 0) ? nP - ELP_CUNIT : (d1 ? nP : nP + ELP_CUNIT);
+    nP |= d1 ? d1 : d2;
+    uint32_t nB = (wB >= 2u * ELP_CUNIT) ? wB - ELP_CUNIT : 0u;
+    uint32_t nY = d2 ? (d2 | ELP_CUNIT) : wY + ELP_CUNIT;
+    if ((wP | (s ? wB : 0u) | (d2 == 0 ? wY : 0u)) & ELP_LBIT)
+        follow_label(slot_so, p, pB, pY, wP, wB, wY, s, d1, nP, nB, nY);
+    if (s) SW(pB) = nB;
+    if (d1) SW(pY) = nY;
+    SW(p) = nP;
+}
+
+// One ring substep of a thread's K anchors.  Anchor q takes its random byte
+// at bit offset bsh[q] of the Philox word w: bit 0 slot (0: the last monomer
+// of P's run, 1: the first monomer of the next run), bits 1-4 table option.
+// Returns the warp's accepted moves (the same value in every lane).
+template <int K, bool PER, int NC, int TABW, int OFFW>
+__device__ __forceinline__ uint32_t substep_ring(uint32_t* slot_so, uint32_t* queue, const int (&base4)[K],
+                                                 const int (&rot4)[K], const int (&clsyz)[K], const int (&xj4)[K],
+                                                 const int (&bsh)[K], int c4, uint32_t w, int L)
+{
+    const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
+    const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t n = 0;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        int xr4 = c4 + rot4[q];
+        if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
+        else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
+        const int p = base4[q] + xr4;
+        int cls = 0;
+        if (PER) {
+            const int x4 = xr4 + xj4[q];
+            cls = clsyz[q] + (x4 == 0 ? 0 : (x4 == 4 * (L - 1) ? 2 : 1));
+        }
+        const int ob = 16 * cls;
+        const uint32_t wP = SW(p);
+        const uint32_t rb = w >> bsh[q];
+        const uint32_t bo = wP & 15;
+        // the next run's word: inside the anchor's radius-1 ball, which no
+        // other anchor of this substep touches (an empty P reads itself)
+        const uint32_t wB = SW(p + offs[ob + bo]);
+        // source bonds (b_{m-1}, b_m): slot 0 uses row (0, b_out(P)) when P's
+        // run holds two or more, else row (0, 0); slot 1 uses row (b_out(P),
+        // next run > 1 ? 0 : b_out(next)).  Rows (0, 0) and (x, 3) hold only
+        // null moves, which covers an empty P, a run of one in slot 0 and a
+        // next run in the halo.
+        const uint32_t s = rb & 1u;
+        const uint32_t v = s ? wB : wP;
+        const bool many = v >= 2u * ELP_CUNIT;
+        const uint32_t src2 = (many != (s != 0)) ? (v & 15u) : 0u;
+        const uint32_t e = tab[((s ? bo : 0u) << 8) | (src2 << 4) | ((rb >> 1) & 15u)];
+        const uint32_t d1 = e & 15u;
+        const uint32_t wY = SW(p + offs[ob + d1]);
+        // accept: the monomer joins the next run (dst2 == 0, which must not
+        // be the halo) or moves to a free site or stays on P (dst1 == 0)
+        const bool ok = e != 0 && ((e >> 4) == 0 ? wY != HWALL : (d1 == 0 || wY == 0));
+        const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) queue[n + __popc(bal & below)] = (uint32_t)p | (e << 18) | (s << 26) | ((uint32_t)cls << 27);
+        n += __popc(bal);
+    }
+    __syncwarp();
+    for (uint32_t b = 0; b < n; b += 32)
+        if (b + lane < n) commit_ring<PER, OFFW>(slot_so, queue[b + lane]);
+    return n;
+}
+
+// One substep of a thread's K anchors with the general move (op: words in
+// their global form, monomer 0's bookkeeping in the chain records, halo
+// words ELP_WALL), for a ring tile whose monomer-0 runs outnumber the slots.
+template <int K, int NC, int WOFFW>
+__device__ __forceinline__ uint32_t substep_general(const Dom& D, const int (&base4)[K], const int (&rot4)[K],
+                                                    const int (&bsh)[K], int c4, uint32_t w)
+{
+    const int* woffs = reinterpret_cast<const int*>(g_smem + WOFFW);
+    uint32_t acc = 0;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        int xr4 = c4 + rot4[q];
+        if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
+        else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
+        acc += (uint32_t)op(D, (base4[q] + xr4) >> 2, woffs, (w >> bsh[q]) & 0xffu);
+    }
+    return acc;
+}
+
+// The K anchors of one thread, one substep, for melts that may hold linear
+// chains (one phase, with the head moves of monomer 0).  Returns accepted
+// moves.  Byte offsets: anchors base4 + 4 xr, colour c4 = 4 c, neighbour
+// offsets at OFFW words; transition table (bytes) at TABW words.
+template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW>
+__device__ __forceinline__ int substep_lin(uint32_t* slot_so, const int (&base4)[K], const int (&rot4)[K],
+                                           const int (&clsyz)[K], const int (&xj4)[K], const int (&bsh)[K],
+                                           const int (&an)[K], int c4, uint32_t w, int L, bool lin, uint32_t t, int d,
+                                           int k, uint2 key)
 {
     const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
     const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
@@ -175,18 +301,15 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
         else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
         p[q] = base4[q] + xr4;
-        int cls = clsyz[q];
+        int cls = 0;
         if (PER) {
             int x4 = xr4 + xj4[q];
-            cls += x4 == 0 ? 0 : (x4 == 4 * (L - 1) ? 2 : 1);
+            cls = clsyz[q] + (x4 == 0 ? 0 : (x4 == 4 * (L - 1) ? 2 : 1));
         }
         ob[q] = 16 * cls;
         wP[q] = SW(p[q]);
         rb[q] = (w >> bsh[q]) & 0xffu;
     }
-    // stage B: the next run (slot 1).  Loaded unconditionally: the index is
-    // inside the anchor's radius-1 ball, which no other anchor of this
-    // substep touches.
     int pB[K];
     uint32_t wB[K];
 #pragma unroll
@@ -194,12 +317,6 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         pB[q] = p[q] + offs[ob[q] + (wP[q] & 15)];
         wB[q] = SW(pB[q]);
     }
-    // stage C: source bonds (b_{m-1}, b_m) and the table option.  Slot 0
-    // (last monomer of P's run) uses row (0, b_out(P)) when the run holds two
-    // or more, else row (0, 0); slot 1 (first monomer of the next run B) uses
-    // row (b_out(P), B's run length > 1 ? 0 : b_out(B)).  Rows (0, 0) and
-    // (x, 0xf) hold only null moves, which covers an empty P (b_out 0, so B
-    // is P itself), a run of one in slot 0 and a next run in the halo.
     uint32_t e[K];
 #pragma unroll
     for (int q = 0; q < K; q++) {
@@ -208,7 +325,6 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         const uint32_t src2 = s ? (c2 ? 0u : (wB[q] & 15)) : (c2 ? bo : 0u);
         e[q] = tab[((s ? bo : 0u) << 8) | (src2 << 4) | ((rb[q] >> 1) & 15)];
     }
-    // stage D: target site P + dst1 (again inside the ball)
     int pY[K];
     uint32_t wY[K];
 #pragma unroll
@@ -216,8 +332,6 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         pY[q] = p[q] + offs[ob[q] + (e[q] & 15)];
         wY[q] = SW(pY[q]);
     }
-    // stage E: accept, label bookkeeping, write.  Store order B, Y, P: when
-    // dst1 == 0 the target is P itself and P's store must come last.
     int acc = 0;
 #pragma unroll
     for (int q = 0; q < K; q++) {
@@ -230,33 +344,11 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
         uint32_t nB = (wB[q] >= 2u * ELP_CUNIT) ? wB[q] - ELP_CUNIT : 0u;
         uint32_t nY = d2 ? (d2 | ELP_CUNIT) : wY[q] + ELP_CUNIT;
         const uint32_t labs = (wP[q] | (s ? wB[q] : 0u) | (join ? wY[q] : 0u)) & ELP_LBIT;
-        if (ok && labs) {
-            // monomer 0 sits in one of the runs this move touches
-            const int src = (wP[q] & ELP_LBIT) ? 0 : ((s && (wB[q] & ELP_LBIT)) ? 1 : 2);
-            const uint32_t lw = src == 0 ? wP[q] : (src == 1 ? wB[q] : wY[q]);
-            const uint32_t slot = (lw >> 5) & 0x7FFu;
-            const uint32_t off0 = slot_off[slot];
-            uint32_t noff;
-            int nl;
-            if (src == 0) {
-                nl = 0; noff = off0;
-                if (s == 0 && off0 == (wP[q] >> ELP_CSHIFT) - 1) { nl = 2; noff = 0; }
-            } else if (src == 1) {
-                if (wB[q] >= 2u * ELP_CUNIT && off0 > 0) { nl = 1; noff = off0 - 1; }
-                else { nl = d1 ? 2 : 0; noff = d1 ? 0 : (nP >> ELP_CSHIFT) - 1; }
-            } else {
-                nl = 2; noff = off0 + 1;
-            }
-            const uint32_t lb = lw & LMASK;
-            if (src == 0) nP &= ~LMASK; else if (src == 1) nB &= ~LMASK; else nY &= ~LMASK;
-            if (nl == 0) nP |= lb; else if (nl == 1) nB |= lb; else nY |= lb;
-            slot_off[slot] = noff;
-            slot_site[slot] = (nl == 0 ? p[q] : (nl == 1 ? pB[q] : pY[q])) >> 2;
-        }
+        if (ok && labs) follow_label(slot_so, p[q], pB[q], pY[q], wP[q], wB[q], wY[q], s, d1, nP, nB, nY);
         if (ok && s) SW(pB[q]) = nB;
         if (ok && d1) SW(pY[q]) = nY;
         if (ok) SW(p[q]) = nP;
-        if (LIN) wP[q] = ok ? nP : wP[q];
+        wP[q] = ok ? nP : wP[q];
         acc += ok ? 1 : 0;
     }
     // linear chains: monomer 0 has no predecessor and moves about monomer 1,
@@ -264,7 +356,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
     // with probability 1/2 (bit 0 of its own Philox word) one option of row
     // (0xf, run length > 1 ? 0 : b_out) -- it leaves to the empty site P - u
     // (its bond to monomer 1 becoming u), or, alone on P, joins the next run
-    if (LIN && lin) {
+    if (lin) {
         const uint8_t* htab = reinterpret_cast<const uint8_t*>(g_smem + HTABW);
 #pragma unroll
         for (int q = 0; q < K; q++) {
@@ -276,12 +368,13 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
             const uint32_t e = htab[((cP >= 2 ? 0u : bo) << 4) | ((h.x >> 1) & 15)];
             if (!e) continue;
             const uint32_t d2 = e >> 4, slot = (w0 >> 5) & 0x7FFu;
+            // monomer 0 of a linear chain is the first of its run: offset 0 stays
             if (cP >= 2) {
                 const int pY = p[q] + offs[ob[q] + ((~d2) & 15u)];
                 if (SW(pY) == 0) {
                     SW(pY) = d2 | (w0 & LMASK) | ELP_CUNIT;
                     SW(p[q]) = (w0 & ~LMASK) - ELP_CUNIT;
-                    slot_site[slot] = pY >> 2;
+                    slot_so[slot] = (slot_so[slot] & 0xFFFFu) | ((uint32_t)(pY >> 2) << 16);
                     acc++;
                 }
             } else {
@@ -290,7 +383,7 @@ __device__ __forceinline__ int substepK(uint32_t* slot_off, int* slot_site, cons
                 if (wB != HWALL) {
                     SW(pB) = (wB + ELP_CUNIT) | (w0 & LMASK);
                     SW(p[q]) = 0;
-                    slot_site[slot] = pB >> 2;
+                    slot_so[slot] = (slot_so[slot] & 0xFFFFu) | ((uint32_t)(pB >> 2) << 16);
                     acc++;
                 }
             }
@@ -309,7 +402,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 {
     using SH = Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, MINB>;
     static_assert(K == 1 || K == 2 || K == 4, "anchors per thread");
-    static_assert(SH::A % 4 == 0 && SH::AT <= THREADS, "threads");
+    static_assert(SH::A % 4 == 0 && SH::AT == THREADS && THREADS % 32 == 0, "every thread owns K anchors");
     static_assert(CAP <= 2048, "slot numbers are 11 bits");
     static_assert((2 * NC) % 4 == 0, "substeps come in groups of four");
     static_assert(THREADS % TX == 0, "tile columns are split evenly over the threads");
@@ -319,9 +412,10 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     int* offs = reinterpret_cast<int*>(g_smem + OFFW);
     uint32_t* col = g_smem + SH::COLW;
     uint32_t* slot_chain = g_smem + SH::SCHW;
-    uint32_t* slot_off = g_smem + SH::SOFW;
-    int* slot_site = reinterpret_cast<int*>(g_smem + SH::SSIW);
+    uint32_t* slot_so = g_smem + SH::SSOW;
     uint32_t* nslots = g_smem + SH::NSLW;
+    uint32_t* ticket = g_smem + SH::TKW;
+    uint32_t* queue = g_smem + SH::QW + (threadIdx.x >> 5) * 32 * K;
     uint4* rnd = reinterpret_cast<uint4*>(g_smem + SH::RNDW);
     const int tid = threadIdx.x;
     const int cx = tid % TX;  // the tile column this thread loads, scans and stores
@@ -337,8 +431,10 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         reinterpret_cast<uint32_t*>(tab)[i] = nobond ? 0u : a.table[i];
     }
     for (int i = tid; i < 64; i += THREADS) g_smem[HTABW + i] = a.table[960 + i];
-    for (int i = tid; i < 27 * 16; i += THREADS) {
-        int cls = i >> 4, b = i & 15;
+    for (int i = tid; i < SH::NOFF; i += THREADS) {
+        // whole box: class (cx, cy, cz) of the anchor on each axis (0 first
+        // plane, 2 last, 1 inside) wraps the offsets; tiles: one class
+        int cls = PER ? (i >> 4) : 13, b = i & 15;
         int dt = elp_bt(b), du = elp_bu(b), dv = elp_bv(b);
         if (PER) {
             int cx = cls % 3, cy = (cls / 3) % 3, cz = cls / 9;
@@ -350,6 +446,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             if (cz == 2 && dv > 0) dv = -(LP - 1);
         }
         offs[i] = 4 * (dt + SX * du + SXY * dv);   // bytes
+        if (!PER) reinterpret_cast<int*>(g_smem + SH::WOFFW)[i] = dt + SX * du + SXY * dv;
     }
     if (!PER)
         for (int i = tid; i < SH::WORDS; i += THREADS) S[i] = HWALL;
@@ -380,20 +477,29 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         clsyz[q] = PER ? (3 * cy + 9 * cz) : 13;
         xj[q] = 4 * NC * j;
     }
-    const bool active = tid < SH::AT;
     const uint32_t step_dev = a.step_dev ? *a.step_dev : 0u;
-    // Whole-box domains run their steps back to back on chip; tiled domains
-    // move their tiles every step, so a launch of several steps takes its
-    // steps one after another over all tiles, with a grid barrier between
-    // steps (the launch is cooperative: all CTAs are resident).
-    const int outer = PER ? 1 : a.nsteps, inner = PER ? a.nsteps : 1;
+    const uint32_t polls = a.wait_polls ? a.wait_polls : WAIT_POLLS;
+    // Whole-box domains run their steps back to back on chip, one work item
+    // per melt.  Tiled domains move their tiles every step: the work items
+    // are (step, tile) pairs, taken in step order from a ticket counter.
+    const int inner = PER ? a.nsteps : 1;
+    const uint32_t total = PER ? (uint32_t)a.nitems : (uint32_t)a.nitems * (uint32_t)a.nsteps;
+    uint32_t next = blockIdx.x;
 
-    for (int so = 0; so < outer; so++) {
-    if (so > 0 && !grid_barrier(a.grid_bar, gridDim.x * (uint32_t)so)) {
-        if (tid == 0) atomicOr(a.error, 4u);
-        break;
-    }
-    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
+    for (;;) {
+        uint32_t tk;
+        if (PER) {
+            tk = next;
+            next += gridDim.x;
+        } else {
+            __syncthreads();   // the previous item is done with the ticket word
+            if (tid == 0) *ticket = atomicAdd(a.flow, 1u);
+            __syncthreads();
+            tk = *ticket;
+        }
+        if (tk >= total) break;
+        const int so = PER ? 0 : (int)(tk / (uint32_t)a.nitems);
+        const int it = PER ? (int)tk : (int)(tk % (uint32_t)a.nitems);
         const uint2 item = a.items[it];
         const BatchJob& J = a.jobs[item.x];
         const int d = (int)item.y;
@@ -408,13 +514,51 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         D.S = S; D.tab = tab; D.rec = rec;
         D.ox = SH::OX; D.sx = SX; D.sxy = SXY; D.L = L;
         D.x0 = 0; D.y0 = 0; D.z0 = 0;
-        int accepted = 0;
-        bool overflow = false;
+        uint32_t accepted = 0;
+        bool overflow = false, skip = false, spill = false;
         int bse[K];   // anchor base byte offsets of this tile (plus its offset sh in the spans)
 #pragma unroll
         for (int q = 0; q < K; q++) bse[q] = base[q];
 
-        for (int st = 0; st < inner && !overflow; st++) {
+        if constexpr (!PER) if (so > 0) {
+            // wait for the tiles of the previous step that overlap this one:
+            // per axis the tile with the same index and, when the origin
+            // moved, the neighbour on the side it moved to (threads 0-7 each
+            // take one of the 2 x 2 x 2 combinations)
+            bool ok = true;
+            if (tid < 8) {
+                const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)so;
+                const uint4 sc = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
+                const uint4 sp = philox(make_uint4(t - 1u, 0, ELP_STREAM_SHIFT, 0), key);
+                const int ci = d % ntx, cj = (d / ntx) % nty, ck = d / ntx / nty;
+                const int ntz = J.ntz;
+                int ii = ci, jj = cj, kk = ck;
+                const int ax = (int)bounded(sc.x, TX), px = (int)bounded(sp.x, TX);
+                const int ay = (int)bounded(sc.y, TY), py = (int)bounded(sp.y, TY);
+                const int az = (int)bounded(sc.z, TZ), pz = (int)bounded(sp.z, TZ);
+                ii += (tid & 1) ? (ax > px ? 1 : 0) : (ax < px ? -1 : 0);
+                jj += (tid & 2) ? (ay > py ? 1 : 0) : (ay < py ? -1 : 0);
+                kk += (tid & 4) ? (az > pz ? 1 : 0) : (az < pz ? -1 : 0);
+                ii += ii < 0 ? ntx : 0; ii -= ii >= ntx ? ntx : 0;
+                jj += jj < 0 ? nty : 0; jj -= jj >= nty ? nty : 0;
+                kk += kk < 0 ? ntz : 0; kk -= kk >= ntz ? ntz : 0;
+                const uint32_t* f = a.done + (size_t)(ii + ntx * (jj + nty * kk)) * a.njobs + item.x;
+                const uint32_t need = (uint32_t)so;   // the previous step announced as so
+                for (uint32_t n = 0; ld_acquire_gpu(f) < need; n++) {
+                    if (n >= polls) { ok = false; break; }
+                    __nanosleep(32);
+                }
+            }
+            if (__syncthreads_or(!ok)) {
+                // a dependency did not finish in time: leave this tile as it
+                // is (its words are not read while they may be written) and
+                // report; the flag below still lets later tiles proceed
+                if (tid == 0) atomicOr(a.error, 4u);
+                skip = true;
+            }
+        }
+
+        for (int st = 0; st < inner && !overflow && !skip; st++) {
             const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)(so + st);
             if (!PER) {
                 const uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
@@ -438,7 +582,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                         for (int r = tid / TX; r < SH::R; r += THREADS / TX) {
                             const int idx = cx + SX * (r % TY) + SXY * (r / TY);
                             const uint32_t wv = S[idx];
-                            if (wv & ELP_LBIT) S[idx] = take_slot<CAP>(wv, idx, rec, nslots, slot_chain, slot_off, slot_site);
+                            if (wv & ELP_LBIT) S[idx] = take_slot<CAP>(wv, idx, rec, nslots, slot_chain, slot_so);
                         }
                     }
                 } else {
@@ -480,10 +624,10 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                             v.w = (unsigned)(p0 + 3) < (unsigned)TX ? v.w : HWALL;
                         }
                         if (!few && ((v.x | v.y | v.z | v.w) & ELP_LBIT)) {
-                            if (v.x & ELP_LBIT) v.x = take_slot<CAP>(v.x, at + 0, rec, nslots, slot_chain, slot_off, slot_site);
-                            if (v.y & ELP_LBIT) v.y = take_slot<CAP>(v.y, at + 1, rec, nslots, slot_chain, slot_off, slot_site);
-                            if (v.z & ELP_LBIT) v.z = take_slot<CAP>(v.z, at + 2, rec, nslots, slot_chain, slot_off, slot_site);
-                            if (v.w & ELP_LBIT) v.w = take_slot<CAP>(v.w, at + 3, rec, nslots, slot_chain, slot_off, slot_site);
+                            if (v.x & ELP_LBIT) v.x = take_slot<CAP>(v.x, at + 0, rec, nslots, slot_chain, slot_so);
+                            if (v.y & ELP_LBIT) v.y = take_slot<CAP>(v.y, at + 1, rec, nslots, slot_chain, slot_so);
+                            if (v.z & ELP_LBIT) v.z = take_slot<CAP>(v.z, at + 2, rec, nslots, slot_chain, slot_so);
+                            if (v.w & ELP_LBIT) v.w = take_slot<CAP>(v.w, at + 3, rec, nslots, slot_chain, slot_so);
                             *reinterpret_cast<uint4*>(S + at) = v;
                         } else if (edge) {
                             *reinterpret_cast<uint4*>(S + at) = v;
@@ -504,8 +648,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                             if (slot < (uint32_t)CAP) {
                                 const int idx = D.ox + x + SX * y + SXY * z;
                                 slot_chain[slot] = (uint32_t)ch;
-                                slot_off[slot] = r.z;
-                                slot_site[slot] = idx;
+                                slot_so[slot] = r.z | ((uint32_t)idx << 16);
                                 S[idx] = (S[idx] & 15) | ELP_LBIT | (slot << 5) | (r.y << ELP_CSHIFT);
                             }
                         }
@@ -522,24 +665,38 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             }
             __syncthreads();
             if (*nslots > (uint32_t)CAP) {
-                // more monomer-0 runs than slots: leave this domain untouched, report
-                if (tid == 0) atomicOr(a.error, 1u);
-                overflow = true;
-                break;
+                if (PER || lin) {
+                    // more monomer-0 runs than slots where the general move
+                    // does not apply: leave this domain untouched, report
+                    if (tid == 0) atomicOr(a.error, 1u);
+                    overflow = true;
+                    break;
+                }
+                // a crowded ring tile: words back to their global form (the
+                // records still hold the runs' lengths and offsets), halo
+                // words to the general move's wall
+                spill = true;
+                for (int sl = tid; sl < CAP; sl += THREADS) {
+                    const int idx = (int)(slot_so[sl] >> 16);
+                    S[idx] = (S[idx] & 15) | ELP_LBIT | (slot_chain[sl] << 5);
+                }
+                for (int i = tid; i < SH::WORDS; i += THREADS)
+                    if (S[i] == HWALL) S[i] = ELP_WALL;
+                __syncthreads();
             }
 #pragma unroll 1
             for (int k = 0; k < 2 * NC; k += 4) {
-                uint4 rw = make_uint4(0, 0, 0, 0);
+                uint4 rw;
                 if (K == 4) {
-                    if (active) rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)tid), key);
+                    rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)gq), key);
                 } else if (SH::PRE) {
-                    if (active) rw = rnd[(k >> 2) * SH::G + gq];
+                    rw = rnd[(k >> 2) * SH::G + gq];
                 } else {
                     // this group's words were drawn during the previous one (or
                     // before the first); G threads now draw the next group's
                     // into the other buffer, read four barriers ago
                     const int cur = (k >> 2) & 1;
-                    if (active) rw = rnd[cur * SH::G + gq];
+                    rw = rnd[cur * SH::G + gq];
                     if (tid < SH::G && k + 4 < 2 * NC)
                         rnd[(cur ^ 1) * SH::G + tid] =
                             philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2) + 1u, (uint32_t)tid), key);
@@ -547,22 +704,35 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 const uint32_t rws[4] = {rw.x, rw.y, rw.z, rw.w};
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++) {
-                    if (active)
-                        accepted += substepK<K, PER, NC, TABW, OFFW, HTABW, LIN>(
-                            slot_off, slot_site, bse, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d,
-                            k + kk, key);
+                    if (!PER && spill)
+                        accepted += substep_general<K, NC, SH::WOFFW>(D, bse, rot, bsh, (int)col[k + kk], rws[kk]);
+                    else if (LIN)
+                        accepted += (uint32_t)substep_lin<K, PER, NC, TABW, OFFW, HTABW>(
+                            slot_so, bse, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d, k + kk,
+                            key);
+                    else {
+                        const uint32_t n = substep_ring<K, PER, NC, TABW, OFFW>(
+                            slot_so, queue, bse, rot, clsyz, xj, bsh, (int)col[k + kk], rws[kk], LP);
+                        accepted += (tid & 31) == 0 ? n : 0u;
+                    }
                     __syncthreads();
                 }
             }
         }
-        if (!overflow) {
-            const uint32_t ns = *nslots;
+        if (spill) {
+            // the halo goes back to the form the slot-table path expects
+            for (int i = tid; i < SH::WORDS; i += THREADS)
+                if (S[i] == ELP_WALL) S[i] = HWALL;
+        }
+        if (!overflow && !skip) {
+            const uint32_t ns = spill ? 0u : *nslots;   // a spilled tile's records are already written
             for (uint32_t sl = tid; sl < ns; sl += THREADS) {
-                const int idx = slot_site[sl];
+                const uint32_t so16 = slot_so[sl];
+                const int idx = (int)(so16 >> 16);
                 const uint32_t wv = S[idx];
                 const uint32_t chain = slot_chain[sl];
                 *reinterpret_cast<uint4*>(rec + ELP_REC_WORDS * (size_t)chain) =
-                    make_uint4(global_site(D, idx), wv >> ELP_CSHIFT, slot_off[sl], 0u);
+                    make_uint4(global_site(D, idx), wv >> ELP_CSHIFT, so16 & 0xFFFFu, 0u);
                 S[idx] = (wv & 15) | ELP_LBIT | (chain << 5);
             }
             __syncthreads();
@@ -600,68 +770,80 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if ((tid & 31) == 0 && v) atomicAdd(J.acc, v);
         }
+        if (!PER) {
+            // announce the tile's step: its stores (lattice and records) are
+            // visible to every CTA that sees the flag (release after the CTA
+            // barrier; readers acquire, then barrier, then load through L2).
+            // A test may hold back one item's first announcement.
+            __syncthreads();
+            if (tid == 0 && !(so == 0 && it + 1 == a.hold_item1)) {
+                __threadfence();
+                st_release_gpu(a.done + it, (uint32_t)so + 1u);
+            }
+        }
     }
+    if (!PER) {
+        // the last CTA out clears the flags and the ticket for the next launch
+        __syncthreads();
+        bool last = false;
+        if (tid == 0) last = atomicAdd(a.flow + 1, 1u) == gridDim.x - 1;
+        if (__syncthreads_or(last)) {
+            for (int i = tid; i < a.nitems; i += THREADS) a.done[i] = 0u;
+            if (tid == 0) {
+                a.flow[0] = 0u;
+                a.flow[1] = 0u;
+            }
+        }
     }
-    if (!PER && a.nsteps > 1) grid_exit(a.grid_bar);
 }
 
 }  // namespace elp
 
 // ---- dispatch ----------------------------------------------------------------
+namespace {
+// Resident CTAs per SM of one kernel, per device (the launch sizes the
+// persistent grid by it); 0 until the first launch on that device asks.
+constexpr int MAX_DEVICES = 64;
+}
+
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int THREADS, int MINB, bool LIN>
 static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 {
     using SH = elp::Shape<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, MINB>;
     auto k = elp::sweep2_kernel<TX, TY, TZ, PER, NC, SX, SXY, CAP, K, THREADS, MINB, LIN>;
+    static std::atomic<int> per_sm[MAX_DEVICES];   // zero-initialised (static storage)
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
     if (l->check_only) {
         // expected monomer-0 runs per domain must stay far inside the slot table
         const double m = l->max_runs_per_domain;
         if (!(PER ? m <= CAP : m + 8.0 * sqrt(m) + 16.0 <= CAP)) return cudaErrorNotSupported;
-        // set the shared-memory limit here, outside any stream capture, once
-        // per device (groups are committed often in the serving loop)
-        static std::atomic<uint32_t> done_devices{0};
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        const uint32_t bit = dev < 32 ? 1u << dev : 0u;
-        if (e == cudaSuccess && !(bit && (done_devices.load() & bit))) {
+        // set the shared-memory limit and size the grid here, outside any
+        // stream capture, once per device (groups are committed often in the
+        // serving loop)
+        if (per_sm[dev].load() < 1) {
             e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::BYTES);
-            if (e == cudaSuccess) done_devices.fetch_or(bit);
+            int n = 0;
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, THREADS, SH::BYTES);
+            if (e != cudaSuccess) return e;
+            if (n < 1) return cudaErrorNotSupported;
+            per_sm[dev].store(n);
         }
-        if (e == cudaSuccess) {
-            const_cast<Sweep2Launch*>(l)->threads_out = THREADS;
-            const_cast<Sweep2Launch*>(l)->smem_out = SH::BYTES;
-        }
-        return e;
+        const_cast<Sweep2Launch*>(l)->threads_out = THREADS;
+        const_cast<Sweep2Launch*>(l)->smem_out = SH::BYTES;
+        return cudaSuccess;
     }
-    int grid = l->args.nitems;
-    if (grid > l->nsm * MINB) grid = l->nsm * MINB;
+    const int resident = l->nsm * (per_sm[dev].load() > 0 ? per_sm[dev].load() : MINB);
+    long work = l->args.nitems;
+    if (!PER) work *= (l->args.nsteps > 0 ? l->args.nsteps : 1);
+    int grid = (int)(work < resident ? work : resident);
     if (grid < 1) return cudaSuccess;
-    if (PER || l->args.nsteps <= 1) {
-        k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
-        return cudaGetLastError();
-    }
-    // tiled, several steps: a cooperative launch (every CTA resident, or an
-    // error) of at most as many CTAs as fit on the device at once
-    static int per_sm = 0;   // resident CTAs per SM of this kernel (same on every device of the pool)
-    if (per_sm < 1) {
-        int n = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, THREADS, SH::BYTES);
-        if (e != cudaSuccess) return e;
-        if (n < 1) return cudaErrorNotSupported;
-        per_sm = n;
-    }
-    if (grid > l->nsm * per_sm) grid = l->nsm * per_sm;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3(THREADS);
-    cfg.dynamicSmemBytes = SH::BYTES;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k, l->args);
+    // tiled launches need no co-residency: a CTA only ever waits for items
+    // with smaller tickets, which CTAs already running hold
+    k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
+    return cudaGetLastError();
 }
 
 // Launch (or, with check_only, test) the specialised kernel for a shape.
@@ -670,7 +852,7 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
 {
     const elp_geometry& g = l->geom;
-    if (l->args.nsteps > 1 && !g.periodic && !l->args.grid_bar) return cudaErrorNotSupported;
+    if (!g.periodic && (!l->args.flow || !l->args.done)) return cudaErrorNotSupported;
 // shape: tile edges, whole box or tiled, colour modulus, shared-memory
 // strides, slot capacity, anchors per thread, threads, min blocks per SM
 #define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_)                                        \

@@ -136,9 +136,9 @@ int main(int argc, char** argv)
     if (cur >= 0) {
         printf("Starting from t=%ld\n", cur);
         if (elp_ptl_requested()) fprintf(stderr, PROG ": ELP_PTL is ignored when resuming\n");
-        memset(&dumper, 0, sizeof(dumper));
         snprintf(file, sizeof(file), "%s/t=%ld_dev=0.res", dir, cur);
         if ((st = elp_load_tuv(ctx, file, (uint64_t)cur))) return die(st);
+        if ((st = elp_dumper_open(&dumper, ctx, dir, 0))) return die(st);
         tmax += cur;
     } else {
         cur = 0;

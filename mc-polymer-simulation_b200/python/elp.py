@@ -40,8 +40,8 @@ class Info(C.Structure):
 
 EXPORTED = [
     "elp_default_spec", "elp_create", "elp_init_melt", "elp_load_chains", "elp_load_tuv", "elp_run",
-    "elp_run_timed", "elp_stream", "elp_sync", "elp_fetch_chains", "elp_write_tuv", "elp_check", "elp_get_info",
-    "elp_get_state", "elp_set_state", "elp_accepted", "elp_destroy", "elp_transition_table",
+    "elp_run_timed", "elp_stream", "elp_sync", "elp_fetch_chains", "elp_fetch_checked", "elp_write_tuv", "elp_check", "elp_get_info",
+    "elp_get_state", "elp_set_state", "elp_accepted", "elp_debug_waits", "elp_destroy", "elp_transition_table",
     "elp_format_tuv", "elp_status_string", "elp_last_error",
     "elp_batch_create", "elp_batch_size", "elp_batch_init_melts", "elp_batch_load_chains", "elp_batch_run",
     "elp_batch_run_timed", "elp_batch_sync", "elp_batch_fetch_chains", "elp_batch_get_state", "elp_batch_check",
@@ -76,12 +76,14 @@ def lib():
         "elp_stream": (vp, [vp]),
         "elp_sync": (i32, [vp]),
         "elp_fetch_chains": (i32, [vp, vp, vp]),
+        "elp_fetch_checked": (i32, [vp, vp, vp, vp]),
         "elp_write_tuv": (i32, [vp, C.c_char_p]),
         "elp_check": (i32, [vp, vp]),
         "elp_get_info": (i32, [vp, vp]),
         "elp_get_state": (i32, [vp, vp, vp]),
         "elp_set_state": (i32, [vp, vp, vp, u64]),
         "elp_accepted": (i32, [vp, vp]),
+        "elp_debug_waits": (i32, [vp, u32, i32]),
         "elp_destroy": (None, [vp]),
         "elp_transition_table": (i32, [vp]),
         "elp_format_tuv": (i32, [i32, i32, i32, vp, vp, vp, C.c_size_t, vp]),
@@ -272,6 +274,14 @@ class Melt:
         check(lib().elp_fetch_chains(self.h, start.ctypes.data, bonds.ctypes.data))
         return start, bonds
 
+    def fetch_checked(self):
+        """(start, bonds, integrity code) from one walk and one scan (elp_fetch_checked)."""
+        start = np.zeros((self.P, 3), dtype=np.int32)
+        bonds = np.zeros((self.P, self.N), dtype=np.uint8)
+        code = C.c_int32()
+        check(lib().elp_fetch_checked(self.h, start.ctypes.data, bonds.ctypes.data, C.byref(code)))
+        return start, bonds, code.value
+
     def write_tuv(self, path):
         check(lib().elp_write_tuv(self.h, path.encode()))
 
@@ -299,6 +309,10 @@ class Melt:
         v = C.c_uint64()
         check(lib().elp_accepted(self.h, C.byref(v)))
         return v.value
+
+    def debug_waits(self, polls=0, hold_tile=-1):
+        """Bound of the waits in tiled multi-step launches (elp_debug_waits)."""
+        check(lib().elp_debug_waits(self.h, polls, hold_tile))
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

@@ -84,8 +84,9 @@ def test_multi_step_launches_equal_single_steps():
     (32, 100, dict(periodic=0, tile=(16, 16, 16)), 5, 10),
 ])
 def test_tiled_multi_step_launches_match_replay(L, N, kw, spl, steps):
-    """Tiled melts run several steps per cooperative launch (grid barrier
-    between steps); every launch boundary still matches the replay."""
+    """Tiled melts run several steps per launch (each tile waiting for the
+    tiles of the previous step it overlaps); every launch boundary still
+    matches the replay."""
     seed = 2000 + L + N
     m = elp.Melt(L=L, N=N, seed=seed, steps_per_launch=spl, **kw)
     m.init_melt()
@@ -198,7 +199,7 @@ def test_l128_matches_replay():
 @pytest.mark.parametrize("L,N,seed,spl,steps", [(128, 1000, 7, 20, 3), (256, 5000, 11, 2, 2)])
 def test_bench_workloads_match_replay_in_multi_step_launches(L, N, seed, spl, steps):
     """The bench's headline and roofline melts at full size, run as the bench
-    runs them (several steps per cooperative launch), equal the replay."""
+    runs them (several steps per launch), equal the replay."""
     m = elp.Melt(L=L, N=N, seed=seed, steps_per_launch=spl)
     m.init_melt()
     r = replay_for(m, seed)
@@ -286,3 +287,27 @@ def test_device_load_of_rings_wrapping_the_box():
     w1, r1 = m.state()
     w2, r2 = m2.state()
     assert np.array_equal(w1, w2) and np.array_equal(r1, r2)
+
+
+def test_fetch_checked_reports_a_corrupted_word():
+    """Every dump of the drop-in programs goes through elp_fetch_checked: a
+    word corrupted between intervals (elp_set_state) is caught at the next
+    dump with efpol's code, not written out."""
+    m = elp.Melt(L=32, N=100, seed=61)
+    m.init_melt()
+    m.run(300)
+    s, b, code = m.fetch_checked()
+    assert code == 0
+    s2, b2 = m.fetch()
+    assert np.array_equal(s, s2) and np.array_equal(b, b2)
+    w, rec = m.state()
+    bad = w.copy()
+    i = int(np.flatnonzero((w != 0) & ((w & 16) == 0))[0])
+    bad[i] = (bad[i] & ~np.uint32(15)) | np.uint32(3)        # not a lattice bond
+    m.set_state(bad, rec, m.step)
+    assert m.fetch_checked()[2] == 4
+    dup = w.copy()
+    j = int(np.flatnonzero(w == 0)[0])
+    dup[j] = w[i]                                            # a run that no ring reaches
+    m.set_state(dup, rec, m.step)
+    assert m.fetch_checked()[2] != 0

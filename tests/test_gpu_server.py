@@ -111,3 +111,37 @@ def test_linear_chain_jobs_same_in_mix_and_plain(tmp_path):
         assert r["status"] == 0 and r["integrity"] == 0 and r["dumps"] == 2
         assert r["checksum"] == plain_checksum(kw, steps), f"job {kw} differs from its single-melt run"
     srv.close()
+
+
+def test_dump_write_failure_fails_the_job(tmp_path):
+    """A dump that cannot be written ends its job with ELP_ERR_IO (the
+    directory is a regular file, so every open fails, also for root)."""
+    blocker = tmp_path / "not_a_dir"
+    blocker.write_text("x")
+    srv = elp.Server(quantum=50)
+    bad = srv.submit(300, dump_interval=100, dump_dir=str(blocker), L=16, N=50, seed=31)
+    good = srv.submit(300, dump_interval=100, dump_dir=str(tmp_path / "ok"), L=16, N=50, seed=32)
+    srv.drain(120)
+    res = {r["id"]: r for r in srv.poll()}
+    assert res[bad]["status"] == elp.ERR_IO
+    assert res[good]["status"] == 0 and res[good]["integrity"] == 0
+    assert sorted(os.listdir(tmp_path / "ok")) == ["t=100_dev=0.res", "t=200_dev=0.res", "t=300_dev=0.res"]
+    srv.close()
+
+
+def test_small_jobs_pass_a_job_waiting_for_memory():
+    """A job that does not fit the budget waits; smaller jobs queued behind it
+    start before it (no head-of-line blocking), and it still runs once the
+    memory frees up."""
+    big = 2 * (64 ** 3 * 4 + 1573 * 16)
+    srv = elp.Server(quantum=50, hbm_budget=int(1.5 * big))
+    first = srv.submit(2000, L=64, N=200, seed=41)            # resident
+    time.sleep(0.05)
+    waiting = srv.submit(100, L=64, N=200, seed=42)           # does not fit beside it
+    small = [srv.submit(100, L=16, N=50, seed=43 + i) for i in range(4)]
+    srv.drain(300)
+    res = {r["id"]: r for r in srv.poll()}
+    assert all(r["status"] == 0 for r in res.values())
+    assert all(res[s]["t_start"] < res[waiting]["t_start"] for s in small)
+    assert res[waiting]["t_start"] >= res[first]["t_done"] - 0.05
+    srv.close()

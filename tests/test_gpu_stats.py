@@ -29,8 +29,8 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 Z = 4.0
 
 
-def gpu_ensemble(L, N, steps, interval, therm, lags, seeds, linear=0):
-    b = elp.Batch([dict(L=L, N=N, seed=s, steps_per_launch=interval, linear=linear) for s in seeds])
+def gpu_ensemble(L, N, steps, interval, therm, lags, seeds, linear=0, **geom):
+    b = elp.Batch([dict(L=L, N=N, seed=s, steps_per_launch=interval, linear=linear, **geom) for s in seeds])
     b.init_melts()
     nseed = len(seeds)
     cms = [[] for _ in range(nseed)]
