@@ -6,19 +6,32 @@ reference efpol's unit, cpupol/efpol_lib.c:123) of the workload.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl elp|reference]
 
 Default workload: the single large ring melt L=128, N=1000, density 1.2
-(2517 rings), seed 7, initialised like the reference's CreatePolymers
-(synthetic: no dataset exists for this path).  The melt runs --spl steps per
-kernel launch (a cooperative launch whose CTAs meet at a grid barrier between
-steps; the same bits as one step per launch).  The lattice (8 MB) is smaller
-than L2, so L2 is flushed before every timed launch (a 256 MB write outside
-the timed events).  After the timed launches the same melt runs
---one-step-launches launches of one step each (`one_step_per_launch` in the
-line: one kernel per MC step).  Extra legs on rank 0: the L=256, N=5000 melt (roofline
-configuration), the reference CPU efpol timed on this host, and the
-end-to-end path through the C ABI with host buffers.
+(2517 rings), seed 7, initialised like the reference's CreatePolymers and
+then RELAXED for --relax steps on the GPU (untimed) before the warm-up and
+the timed steps, so that the timed steps see the dense melt a production run
+of 10^5 steps spends its time in, not the collapsed initial melt (synthetic:
+no dataset exists for this path).  The melt runs --spl steps per kernel
+launch (a persistent launch whose tiles of consecutive steps wait only for
+the tiles they overlap; the same bits as one step per launch).  The lattice
+(8 MB) is smaller than L2, so L2 is flushed before every timed launch (a
+256 MB write outside the timed events).  After the timed launches the same
+melt runs --one-step-launches launches of one step each
+(`one_step_per_launch` in the line: one kernel per MC step).
+
+Extra legs (one GPU only): the L=256, N=5000 melt (roofline configuration,
+relaxed --l256-relax steps), the reference CPU efpol timed on this host from
+the same relaxed melt (read by the reference's own ReadLatticeFile), the
+reference's own GPU engine gpupol3 on this GPU, the end-to-end path through
+the C ABI with host buffers, the 512-replica ensemble (batched vs plain,
+from relaxed members) and the served stream.
 
 --gpus N runs N independent replicas (one process per GPU, seeds offset by
 rank); there is no data-path collective -- replicas only.
+
+--impl reference times the reference's own efpol (compiled from its sources
+into oracle/_ref) on all host cores, on the same relaxed melt: the relaxed
+configuration is produced on the GPU by this engine (untimed, as a run's
+earlier dump would be) and read by the reference from its TUV file.
 """
 from __future__ import annotations
 
@@ -157,27 +170,69 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(w, steps, threads=1):
-    """Reference efpol (built from the reference sources into oracle/_ref) timed
-    on this host: `threads` independent processes, each `steps` MC steps."""
+def ref_binary():
+    """The reference efpol's bench driver (oracle/_ref, compiled from the
+    reference sources) or, where the reference was not built, the oracle's
+    restatement of it."""
     ref = os.path.join(REPO, "oracle", "_ref", "ref_bench")
-    kind = "reference"
-    if not os.path.exists(ref):
-        ref = os.path.join(REPO, "oracle", "efpol_port")
-        kind = "port"
-        if not os.path.exists(ref):
-            subprocess.run(["make", "-C", os.path.join(REPO, "oracle")], check=True, stdout=subprocess.DEVNULL)
+    if os.path.exists(ref):
+        return ref, "reference"
+    port = os.path.join(REPO, "oracle", "efpol_port")
+    if not os.path.exists(port):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle")], check=True, stdout=subprocess.DEVNULL)
+    return port, "port"
+
+
+def cpu_baseline(w, steps, threads=1, tuv=None, start_desc="CreatePolymers initial melt"):
+    """Reference efpol timed on this host: `threads` independent processes,
+    each `steps` MC steps of the melt, from the TUV file `tuv` (read by the
+    reference's ReadLatticeFile) or from CreatePolymers."""
+    ref, kind = ref_binary()
+    if tuv and kind != "reference":
+        tuv, start_desc = None, "CreatePolymers initial melt (the restatement reads no TUV)"
     t0 = time.perf_counter()
-    procs = [subprocess.Popen([ref, str(w["L"]), str(w["N"]), str(w["density"]), str(w["seed"] + i), str(steps)],
-                              stdout=subprocess.PIPE, text=True) for i in range(threads)]
-    outs = [json.loads(p.communicate()[0].strip().splitlines()[-1]) for p in procs]
+    procs = [subprocess.Popen([ref, str(w["L"]), str(w["N"]), str(w["density"]), str(w["seed"] + i), str(steps)]
+                              + ([tuv] if tuv else []), stdout=subprocess.PIPE, text=True) for i in range(threads)]
+    outs = []
+    for p in procs:
+        o = p.communicate()[0]
+        if p.returncode != 0:
+            raise RuntimeError(f"{ref} exited {p.returncode}")
+        outs.append(json.loads(o.strip().splitlines()[-1]))
     wall = time.perf_counter() - t0
     moves = sum(o["moves"] for o in outs)
     # processes run concurrently; each times its own DoMCStep window
     rate = moves / max(o["seconds"] for o in outs)
     return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{steps} MC steps of L={w['L']} N={w['N']} per process, {threads} process(es), "
-                      f"{moves:.3g} attempted moves in {wall:.2f} s"}
+            "sample": f"{steps} MC steps of L={w['L']} N={w['N']} per process from the {start_desc}, "
+                      f"{threads} process(es), {moves:.3g} attempted moves in {wall:.2f} s"}
+
+
+def occupied_fraction(m):
+    import numpy as np
+    w, _ = m.state()
+    return float(np.count_nonzero(w)) / w.size
+
+
+def relaxed_melt(elp, w, seed, dev, spl, relax):
+    """The workload's melt: CreatePolymers' initial melt, then `relax` steps
+    on the GPU (untimed)."""
+    m = elp.Melt(L=w["L"], N=w["N"], seed=seed, device=dev, steps_per_launch=spl)
+    m.init_melt()
+    if relax > 0:
+        m.run(relax)
+    m.sync()
+    return m
+
+
+def common_config(w, relax):
+    """The `config` both arms print (identical keys and values)."""
+    return {"workload": f"ring melt L={w['L']} N={w['N']} density={w['density']} P={npol(w)} seed={w['seed']}, "
+                        f"relaxed: {relax} steps from CreatePolymers",
+            "L": w["L"], "N": w["N"], "P": npol(w), "density": w["density"], "seed": w["seed"],
+            "sites": w["L"] ** 3, "monomers": w["N"] * npol(w), "relax_steps": relax,
+            "l2": "GPU arm: flushed before every timed launch (256 MB write on the melt's stream, queued before the "
+                  "start event), the lattice staying in L2 inside a launch; CPU arm: host caches, no flush"}
 
 
 def replica_seed(w, rank):
@@ -205,6 +260,8 @@ def max_over_ranks(x, world):
 
 
 def run_elp(args, rank, world):
+    import tempfile
+
     import torch
     import elp
 
@@ -215,46 +272,49 @@ def run_elp(args, rank, world):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
     spl = max(1, args.spl)
-    m = elp.Melt(L=w["L"], N=w["N"], seed=replica_seed(w, rank), device=dev, steps_per_launch=spl)
-    m.init_melt()
+    m = relaxed_melt(elp, w, replica_seed(w, rank), dev, spl, args.relax)
+    occ = occupied_fraction(m)
     m.run(args.warmup)
     m.sync()
     info = m.info()
+    a0 = m.accepted()
 
     barrier(world)
     with ClockSampler(dev) as clk:
         times = timed_steps(m, torch, flush, dev, args.steps, spl)
     total_ms = max_over_ranks(sum(times), world)
     barrier(world)
+    accepted = m.accepted() - a0
     value = world * args.steps * M / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
     assert m.check() == 0, "integrity check failed after the timed run"
+    extras = rank == 0 and world == 1 and not args.no_extras
     # the same melt with one kernel launch per MC step (every launch flushed
     # from L2 first), beside the multi-step launches of the headline
     one = None
-    if args.one_step_launches > 0 and not args.no_extras:
+    if args.one_step_launches > 0 and extras:
         ot = timed_steps(m, torch, flush, dev, args.one_step_launches, 1)
-        one_ms = max_over_ranks(sum(ot), world) / len(ot)
-        one = {"ms_per_step": one_ms, "value": world * M / (one_ms / 1e3), "unit": UNIT, "launches": len(ot),
+        one_ms = sum(ot) / len(ot)
+        one = {"ms_per_step": one_ms, "value": M / (one_ms / 1e3), "unit": UNIT, "launches": len(ot),
                "l2": "flushed before every launch"}
         assert m.check() == 0, "integrity check failed after the one-step launches"
 
     peak, peak_kind = measured_peak()
     achieved = algo_bytes(w) / (ms_per_step / 1e3) / 1e9
     tr = profile_traffic(args.workload, spl)
+    cfg = common_config(w, args.relax)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference CreatePolymers initial melt)",
-        "config": {"workload": f"ring melt L={w['L']} N={w['N']} density={w['density']} P={npol(w)} "
-                               f"seed={w['seed']}, {spl} steps per sweep launch",
-                   "steps_per_launch": spl,
-                   "L": w["L"], "N": w["N"], "P": npol(w), "sites": w["L"] ** 3, "monomers": M,
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference CreatePolymers initial melt, relaxed on "
+                                                      "the GPU before timing)",
+        "config": dict(cfg, parallelism=f"replicas x{world}"),
+        "kernel": {"steps_per_launch": spl,
                    "geometry": {"periodic": info.periodic, "tile": list(info.tile), "ncol": info.ncol,
-                                "domains": info.domains, "threads": info.threads},
-                   "l2": f"flushed before every timed launch of {spl} steps (256 MB write on the melt's stream, "
-                         "queued before the start event); inside a launch the lattice stays in L2 between steps",
-                   "parallelism": f"replicas x{world}"},
+                                "domains": info.domains, "threads": info.threads}},
+        "state": {"occupied_site_fraction": occ,
+                  "accepted_moves_per_s": accepted / (total_ms / 1e3) if world == 1 else None,
+                  "acceptance": accepted / (args.steps * M)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": spl * algo_bytes(w),
@@ -271,9 +331,14 @@ def run_elp(args, rank, world):
     if ic:
         line["issue_roofline"] = ic
 
-    if rank == 0 and not args.no_extras:
+    if extras:
+        with tempfile.TemporaryDirectory(prefix="elp_bench_") as tmp:
+            tuv = os.path.join(tmp, f"relaxed_L{w['L']}.res")
+            m.write_tuv(tuv)
+            line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps, 1, tuv, f"relaxed melt after {m.step} steps")
         line["e2e"] = e2e_leg(elp, w, dev, args)
-        line["cpu_baseline"] = cpu_baseline(w, args.cpu_steps)
+        if not args.no_gpu_reference:
+            line["gpu_reference"] = gpu_reference_leg(w, ms_per_step, args.gp3_interval)
         if args.workload != "L256" and not args.no_l256:
             line["L256"] = l256_leg(elp, torch, dev, flush, args, (clk_s or {}).get("sm_mhz"))
         if not args.no_batched:
@@ -285,14 +350,13 @@ def run_elp(args, rank, world):
 
 def e2e_leg(elp, w, dev, args):
     """Through the C ABI with host buffers: per bench step, load the rings from
-    pinned host memory (H2D), run one dump interval, fetch them back (D2H)."""
-    import numpy as np
+    pinned host memory (H2D), run one dump interval, fetch them back (D2H).
+    Starts from the relaxed melt."""
     import torch
 
     interval = args.e2e_interval
     P, N = npol(w), w["N"]
-    m = elp.Melt(L=w["L"], N=N, seed=w["seed"], device=dev, steps_per_launch=max(1, args.spl))
-    m.init_melt()
+    m = relaxed_melt(elp, w, w["seed"], dev, max(1, args.spl), args.relax)
     m.run(args.warmup)
     start_t = torch.empty((P, 3), dtype=torch.int32).pin_memory()
     bonds_t = torch.empty((P, N), dtype=torch.uint8).pin_memory()
@@ -337,7 +401,8 @@ def e2e_leg(elp, w, dev, args):
             "bytes_per": f"call cycle (load, {interval} MC steps, fetch): the chains go in and come back once per cycle",
             "ms_per_call": 1e3 * dt / reps,
             "parts_ms_median": {k: 1e3 * sorted(v)[len(v) // 2] for k, v in parts.items()},
-            "path": "elp_load_chains(host) + elp_run(interval) + elp_fetch_chains(host), wall clock"}
+            "path": "elp_load_chains(host) + elp_run(interval) + elp_fetch_chains(host), wall clock, from the "
+                    f"melt relaxed {args.relax} steps"}
 
 
 def timed_steps(m, torch, flush, dev, nsteps, spl=1):
@@ -364,18 +429,24 @@ def l256_leg(elp, torch, dev, flush, args, clock_mhz):
     w = WORKLOADS["L256"]
     M = w["N"] * npol(w)
     spl = max(1, args.l256_spl)
-    m = elp.Melt(L=w["L"], N=w["N"], seed=w["seed"], device=dev, steps_per_launch=spl)
-    m.init_melt()
+    m = relaxed_melt(elp, w, w["seed"], dev, spl, args.l256_relax)
+    occ = occupied_fraction(m)
     m.run(3 * spl)
     m.sync()
     nsteps = max(3 * spl, args.steps // 2 // spl * spl)
+    a0 = m.accepted()
     times = timed_steps(m, torch, flush, dev, nsteps, spl)
+    acc = m.accepted() - a0
     ms = sum(times) / nsteps
+    assert m.check() == 0
     peak, _ = measured_peak()
     achieved = algo_bytes(w) / (ms / 1e3) / 1e9
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    out = {"workload": f"ring melt L=256 N=5000 P=4027 seed=11, {spl} steps per sweep launch", "value": M / (ms / 1e3),
-           "unit": UNIT, "ms_per_step": ms, "steps": nsteps, "steps_per_launch": spl,
+    out = {"workload": f"ring melt L=256 N=5000 P=4027 seed=11, relaxed: {args.l256_relax} steps from "
+                       f"CreatePolymers, {spl} steps per sweep launch",
+           "value": M / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": nsteps, "steps_per_launch": spl,
+           "state": {"occupied_site_fraction": occ, "accepted_moves_per_s": acc / (sum(times) / 1e3),
+                     "acceptance": acc / (nsteps * M)},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "algorithmic_bytes_per_launch": spl * algo_bytes(w),
                         "traffic": profile_traffic("L256", spl)}}
@@ -383,6 +454,44 @@ def l256_leg(elp, torch, dev, flush, args, clock_mhz):
     if ic:
         out["issue_roofline"] = ic
     return out
+
+
+def gpu_reference_leg(w, ms_per_step, interval, timeout=900):
+    """The reference's own GPU engine, gpupol3 (gpupol2/ with 4^3 cells and
+    32^3 blocks), built from its unmodified sources for sm_100a
+    (oracle/Makefile target _ref/gpupol3_cuda_ring: -gencode for sm_100a,
+    the system host compiler), run on this GPU on the same box, ring length,
+    density and seed, and timed by its own progress line: "MF/s" = lattice
+    sites x steps per second (gpupol2/gpupol2.c:58), over intervals of
+    `interval` steps that end with its synchronous dump
+    (gpupol2/gpupol_cuda.cu:52-76).  Its move set is not efpol's (three move
+    kinds on 1-byte site words, gpupol2/ringpol3.cu:92-219), so the
+    comparison is per lattice site and step, the unit it reports; per step it
+    makes 51 x 4 move attempts per 64-site cell (3.19 per site) against two
+    anchor visits per site here."""
+    exe = os.path.join(REPO, "oracle", "_ref", "gpupol3_cuda_ring")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/gpupol3_cuda_ring not built (set ELP_REFERENCE and make -C oracle ref)"}
+    import re
+    import tempfile
+    L = w["L"]
+    with tempfile.TemporaryDirectory(prefix="elp_gp3_") as tmp:
+        cmd = [exe, str(w["N"]), str(2 * interval), str(w["seed"]), os.path.join(tmp, "run"), str(w["density"]), "0",
+               str(interval), str(L), str(L), str(L)]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"gpupol3 did not finish {2 * interval} steps in {timeout} s"}
+    rates = [float(x) for x in re.findall(r"at ([0-9.]+) MF/s", r.stdout.replace("\r", "\n"))]
+    if r.returncode != 0 or not rates:
+        return {"unavailable": f"gpupol3 exited {r.returncode}: {(r.stdout + r.stderr)[-300:]}"}
+    ref = rates[-1] * 1e6                       # sites x steps / s, the last interval (the first pays start-up)
+    ours = L ** 3 / (ms_per_step / 1e3)
+    return {"engine": "reference gpupol3_cuda_ring (gpupol2/, LCELL=4), unmodified sources built for sm_100a",
+            "workload": f"L={L} N={w['N']} density={w['density']} seed={w['seed']}, {2 * interval} steps, "
+                        f"its own MF/s over the last interval of {interval} steps (synchronous dump included)",
+            "mf_per_s": rates, "sites_steps_per_s": ref, "ours_sites_steps_per_s": ours, "ours_over_reference": ours / ref,
+            "move_attempts_per_site_step": {"gpupol3": 51 * 4 / 64, "ours": 2.0}}
 
 
 # ---- batched ensemble (512 replicas) ------------------------------------------
@@ -416,35 +525,37 @@ def ensemble_mix(n=512, first_seed=1000, density=1.2):
     return out
 
 
-def cpu_ensemble(mix, target_moves=1e8, max_procs=None):
+def cpu_ensemble(mix, target_moves=1e8, max_procs=None, tuvs=None):
     """The reference efpol on the ensemble's members it can run (L a power of
     two: 16, 32, 64), one process per host core at once, each a bounded sample
     of about target_moves attempted moves; the aggregate is the sum of the
-    processes' own rates (they run concurrently)."""
-    ref = os.path.join(REPO, "oracle", "_ref", "ref_bench")
-    kind = "reference"
-    if not os.path.exists(ref):
-        ref = os.path.join(REPO, "oracle", "efpol_port")
-        kind = "port"
-        if not os.path.exists(ref):
-            subprocess.run(["make", "-C", os.path.join(REPO, "oracle")], check=True, stdout=subprocess.DEVNULL)
+    processes' own rates (they run concurrently).  tuvs maps a member's seed
+    to a TUV file of its relaxed state (read by the reference's
+    ReadLatticeFile); members without one start from CreatePolymers."""
+    ref, kind = ref_binary()
     members = [m for m in mix if m["L"] in (16, 32, 64)]
     nproc = min(len(members), max_procs or os.cpu_count() or 1)
     members = members[:nproc]
     procs = []
+    relaxed = 0
     for m in members:
         M = m["N"] * max(1, int(m["density"] * m["L"] ** 3 / m["N"] + 0.5))
         steps = max(10, int(target_moves / M))
-        procs.append(subprocess.Popen([ref, str(m["L"]), str(m["N"]), str(m["density"]), str(m["seed"]), str(steps)],
-                                      stdout=subprocess.PIPE, text=True))
+        tuv = (tuvs or {}).get(m["seed"]) if kind == "reference" else None
+        relaxed += 1 if tuv else 0
+        procs.append(subprocess.Popen([ref, str(m["L"]), str(m["N"]), str(m["density"]), str(m["seed"]), str(steps)]
+                                      + ([tuv] if tuv else []), stdout=subprocess.PIPE, text=True))
     outs = [json.loads(p.communicate()[0].strip().splitlines()[-1]) for p in procs]
     rate = sum(o["moves"] / o["seconds"] for o in outs)
     return {"value": rate, "unit": UNIT, "cores": nproc, "kind": kind,
             "sample": f"the first {nproc} members with L in {{16,32,64}} (efpol rounds L up to a power of two, so "
-                      f"L=24/48 do not run), about {target_moves:.0e} attempted moves each, one process per core"}
+                      f"L=24/48 do not run), about {target_moves:.0e} attempted moves each, one process per core, "
+                      f"{relaxed} of them from the members' relaxed states"}
 
 
 def batched_leg(elp, dev, args):
+    import tempfile
+
     mix = ensemble_mix(args.replicas)
     tuned = {}
     for L in sorted({m["L"] for m in mix}):
@@ -459,15 +570,19 @@ def batched_leg(elp, dev, args):
     moves = sum(sp["N"] * max(1, int(sp["density"] * sp["L"] ** 3 / sp["N"] + 0.5)) for sp in specs)
     b = elp.Batch(specs, device=dev)
     b.init_melts()
+    b.run(args.batch_relax)            # relax every member (untimed)
+    b.sync()
+    relaxed = [b.state(j) for j in range(len(specs))]
+    step0 = args.batch_relax
     b.run(args.batch_warmup)
     b.sync()
     bms = b.run_timed(args.batch_steps)
     batched = moves * args.batch_steps / (bms / 1e3)
-    # plain kernel, same mix, one replica at a time
+    # plain kernel, same mix, one replica at a time, from the same relaxed states
     pms, check_idx, same = 0.0, list(range(0, len(specs), max(1, len(specs) // 16))), True
     for j, sp in enumerate(specs):
         m = elp.Melt(**sp)
-        m.init_melt()
+        m.set_state(relaxed[j][0], relaxed[j][1], step0)
         m.run(args.batch_warmup)
         pms += m.run_timed(args.batch_steps)
         if j in check_idx:
@@ -476,19 +591,35 @@ def batched_leg(elp, dev, args):
             same = same and bool((wa == wb).all() and (ra == rb).all())
         m.close()
     plain = moves * args.batch_steps / (pms / 1e3)
+    occ = sum(int((r[0] != 0).sum()) for r in relaxed) / sum(r[0].size for r in relaxed)
+    # the reference on its members, from their relaxed states
+    with tempfile.TemporaryDirectory(prefix="elp_ens_") as tmp:
+        tuvs = {}
+        for j, sp in enumerate(specs):
+            if sp["L"] in (16, 32, 64) and len(tuvs) < (os.cpu_count() or 1):
+                mm = elp.Melt(**sp)
+                mm.set_state(relaxed[j][0], relaxed[j][1], step0)
+                path = os.path.join(tmp, f"m{sp['seed']}.res")
+                mm.write_tuv(path)
+                mm.close()
+                tuvs[sp["seed"]] = path
+        cpu = cpu_ensemble(mix, tuvs=tuvs)
     b.close()
     # tiled groups take one step per launch inside a batch of several groups
     geoms = {str(L): {"periodic": t["periodic"], "tile": list(t["tile"]), "ncol": t["ncol"],
                       "steps_per_launch": t["steps_per_launch"] if t["periodic"] == 1 else 1}
              for L, t in tuned.items()}
     return {"workload": f"{len(specs)} ring melts, L uniform on {{16,24,32,48,64}}, N log-uniform on [50,1000], "
-                        f"density 1.2, seeds 1000..{999 + len(specs)}",
+                        f"density 1.2, seeds 1000..{999 + len(specs)}, relaxed: {args.batch_relax} steps from "
+                        f"CreatePolymers",
             "monomers": moves, "steps": args.batch_steps, "warmup": args.batch_warmup,
+            "occupied_site_fraction": occ,
             "batched": {"value": batched, "unit": UNIT, "ms": bms},
-            "plain": {"value": plain, "unit": UNIT, "ms": pms, "how": "each replica alone, same specs, sequential"},
+            "plain": {"value": plain, "unit": UNIT, "ms": pms,
+                      "how": "each replica alone, same specs, sequential, from the same relaxed state"},
             "speedup": batched / plain, "batched_equals_plain_bits": same,
             "replicas_compared": len(check_idx), "autotuned_geometry": geoms,
-            "cpu_reference": cpu_ensemble(mix)}
+            "cpu_reference": cpu}
 
 
 # ---- served stream ------------------------------------------------------------
@@ -497,9 +628,9 @@ def served_leg(elp, dev, args):
     the ensemble mix plus 5 % L=128/N=1000 jobs; latency = done - submitted."""
     import random
     import threading
-    full = args.served_full
-    rate, dur = 200.0, (60.0 if full else args.served_seconds)
-    steps, dump = (10000, 1000) if full else (args.served_steps, args.served_dump)
+    rate, dur = 200.0, args.served_seconds
+    steps, dump = args.served_steps, args.served_dump
+    full = (dur, steps, dump) == (60.0, 10000, 1000)
     rng = random.Random(20261203)
     mix = ensemble_mix(4096, first_seed=50000)
     arrivals, t = [], 0.0
@@ -555,7 +686,28 @@ def served_leg(elp, dev, args):
             "quantum": args.served_quantum}
 
 
+def reference_start(w, relax, tmpdir):
+    """The relaxed melt the reference arm starts from: produced on the GPU by
+    this engine (untimed), written as a TUV file.  Without a GPU the
+    reference starts from its own CreatePolymers melt."""
+    try:
+        import torch
+        if not torch.cuda.is_available() or relax <= 0:
+            return None, "CreatePolymers initial melt (no GPU to relax it)" if relax > 0 else "CreatePolymers"
+        sys.path.insert(0, os.path.join(REPO, "mc-polymer-simulation_b200", "python"))
+        import elp
+        m = relaxed_melt(elp, w, w["seed"], 0, 20, relax)
+        path = os.path.join(tmpdir, f"relaxed_L{w['L']}.res")
+        m.write_tuv(path)
+        m.close()
+        return path, f"melt relaxed {relax} steps on the GPU (untimed), read by the reference's ReadLatticeFile"
+    except Exception as e:   # the arm still runs, from the reference's own initial melt
+        return None, f"CreatePolymers initial melt (relaxing failed: {e})"
+
+
 def run_reference(args, rank, world):
+    import tempfile
+
     if rank != 0:
         return None
     w = WORKLOADS[args.workload]
@@ -563,21 +715,24 @@ def run_reference(args, rank, world):
     steps_per = max(1, args.ref_steps)
     tot_moves, tot_wall = 0.0, 0.0
     cb = None
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(w, steps_per, threads)
-        if i >= args.warmup:
-            moves = threads * steps_per * w["N"] * npol(w)
-            tot_moves += moves
-            tot_wall += moves / cb["value"]
+    with tempfile.TemporaryDirectory(prefix="elp_ref_") as tmp:
+        tuv, desc = reference_start(w, args.relax, tmp)
+        for i in range(args.warmup + args.steps):
+            cb = cpu_baseline(w, steps_per, threads, tuv, desc)
+            if i >= args.warmup:
+                moves = threads * steps_per * w["N"] * npol(w)
+                tot_moves += moves
+                tot_wall += moves / cb["value"]
     value = tot_moves / tot_wall
     cb["value"] = value
+    cfg = common_config(w, args.relax)
     return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_wall / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic (reference CreatePolymers initial melt)",
-            "config": {"workload": f"ring melt L={w['L']} N={w['N']} density={w['density']} P={npol(w)}; each step "
-                                   f"= {steps_per} MC steps per process on {threads} host cores",
-                       "L": w["L"], "N": w["N"], "P": npol(w)},
+            "data": "synthetic (reference CreatePolymers initial melt, relaxed on the GPU before timing)",
+            "config": dict(cfg, parallelism=f"replicas x{world}"),
+            "reference_step": f"{steps_per} MC steps of the reference's DoMCStep per process, {threads} processes "
+                              f"at once on {threads} host cores, from the {desc}",
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -589,6 +744,10 @@ def main():
     ap.add_argument("--impl", default="elp", choices=["elp", "reference"])
     ap.add_argument("--workload", default="L128", choices=sorted(WORKLOADS))
     ap.add_argument("--spl", type=int, default=20, help="MC steps per sweep launch (headline workload and e2e)")
+    ap.add_argument("--relax", type=int, default=2000,
+                    help="untimed GPU steps from CreatePolymers before the headline melt is timed (both arms)")
+    ap.add_argument("--l256-relax", type=int, default=5000)
+    ap.add_argument("--batch-relax", type=int, default=2000)
     ap.add_argument("--l256-spl", type=int, default=10, help="MC steps per sweep launch of the L=256 leg")
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--ref-steps", type=int, default=8)
@@ -599,14 +758,16 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-l256", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-gpu-reference", action="store_true")
+    ap.add_argument("--gp3-interval", type=int, default=5000,
+                    help="steps per timed interval of the reference gpupol3 leg (it runs two)")
     ap.add_argument("--replicas", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--batch-warmup", type=int, default=20)
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--served-full", action="store_true")
-    ap.add_argument("--served-seconds", type=float, default=5.0)
-    ap.add_argument("--served-steps", type=int, default=1000)
-    ap.add_argument("--served-dump", type=int, default=250)
+    ap.add_argument("--served-seconds", type=float, default=60.0)
+    ap.add_argument("--served-steps", type=int, default=10000)
+    ap.add_argument("--served-dump", type=int, default=1000)
     ap.add_argument("--served-quantum", type=int, default=50)
     args = ap.parse_args()
     if args.warmup < 3:
