@@ -147,15 +147,20 @@ elp_status elp_get_info(const elp_ctx* ctx, elp_info* info);
  * quota, a latency-critical loop that cannot take an allocation's implicit
  * device synchronisation.  It runs the checks of elp_check on a melt the
  * caller holds on the device (d_words[L^3] site words, d_records[4*P], the
- * layout of elp_get_state) and returns the same code in *code.  Its scratch
- * memory is a static device array of ELP_NOALLOC_MAX_SITES visit counters and
+ * layout of elp_get_state) and returns the same code in *code.  Ring melts
+ * only: the walk follows rings, so a melt of linear chains gets code 4 (a
+ * false failure); check linear melts with elp_check.  Its scratch memory is
+ * a static device array of ELP_NOALLOC_MAX_SITES visit counters and
  * ELP_NOALLOC_MAX_RINGS ring statuses (about 1.5 MB, held by every GPU that
  * loads the library until the process exits); larger melts are rejected with
  * ELP_ERR_ARG.  The first call on a device looks up the array's device
- * address once.  All calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller.  `stream` is a cudaStream_t
- * (NULL: the default stream); the call blocks until the result is on the
- * host. */
+ * address once and keeps it for the life of the process; make that first
+ * call before any stream capture.  A process that resets the device
+ * (cudaDeviceReset) must not call this entry point again, since the module
+ * may then sit at another address.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  `stream` is
+ * a cudaStream_t (NULL: the default stream); the call blocks until the
+ * result is on the host. */
 #define ELP_NOALLOC_MAX_SITES 262144u   /* L <= 64 */
 #define ELP_NOALLOC_MAX_RINGS 131072u
 elp_status elp_check_noalloc(const uint32_t* d_words, const uint32_t* d_records, int32_t L, int32_t N, int32_t P,

@@ -13,6 +13,10 @@
 // contents; the parts that must start at zero are cleared on the caller's
 // stream before the kernels run.  Calls that overlap on the GPU (two streams,
 // or two threads) race on the array and must be serialised by the caller.
+// The walk follows rings: a melt of linear chains gets code 4.  The array's
+// device address is looked up once per device and kept; after a device reset
+// (cudaDeviceReset) the module can come back at another address, so a
+// process that resets a device must not call this entry point again.
 #include <cuda_runtime.h>
 #include <string.h>
 
