@@ -11,8 +11,8 @@ then RELAXED for --relax steps on the GPU (untimed) before the warm-up and
 the timed steps, so that the timed steps see the dense melt a production run
 of 10^5 steps spends its time in, not the collapsed initial melt (synthetic:
 no dataset exists for this path).  The melt runs --spl steps per kernel
-launch (a persistent launch whose tiles of consecutive steps wait only for
-the tiles they overlap; the same bits as one step per launch).  The lattice
+launch (a cooperative launch whose CTAs meet at a grid barrier between
+steps; the same bits as one step per launch).  The lattice
 (8 MB) is smaller than L2, so L2 is flushed before every timed launch (a
 256 MB write outside the timed events).  After the timed launches the same
 melt runs --one-step-launches launches of one step each

@@ -55,10 +55,8 @@ typedef struct elp_job_spec {
     int32_t tile[3];          /* tiled domain edges, 0 = auto */
     int32_t ncol;             /* colour modulus, 0 = auto */
     int32_t device;           /* CUDA device ordinal */
-    int32_t steps_per_launch; /* steps per kernel launch (>=1); tiled domains: the launch's tiles of
-                                 consecutive steps run as a dataflow, each tile waiting only for the
-                                 tiles of the previous step that overlap it.  Any value gives the
-                                 same bits. */
+    int32_t steps_per_launch; /* steps per kernel launch (>=1); tiled domains: a cooperative launch with a
+                                 grid barrier between steps.  Any value gives the same bits. */
     int32_t kernel;           /* 0 auto (specialised when the shape has one), 1 generic */
     int32_t linear;           /* 0 ring polymers (efpol_ring), 1 linear chains (efpol_lin): the last
                                * bond of every chain is the end marker 0xf ('f' in TUV files).
@@ -141,6 +139,21 @@ elp_status elp_check(elp_ctx* ctx, int32_t* code);
 
 elp_status elp_get_info(const elp_ctx* ctx, elp_info* info);
 
+/* Time factor of a domain geometry against the reference efpol's clock.
+ * Tile walls reject the moves that would cross them, as gpupol's block walls
+ * do (gpupol2/ringpol3.cu:58-76).  The walls move every step, so the
+ * equilibrium is efpol's, but the clock runs slower: after t steps a tiled
+ * melt has moved as far as efpol after f*t steps (centre-of-mass MSD).
+ * f = 1 for a whole-box melt (periodic = 1); for the tile shapes the engine
+ * picks, f is the value measured against reference efpol ensembles (rings of
+ * N = 100 at L = 64, density 1.2, steps 15000-50000); 0 for a shape not
+ * measured.  The reference records its own engines' clocks the same way, as
+ * the time factor of their Executable in scripts/ne_list.dat
+ * (analysis/mode_init.c:699-727): the drop-in programs name a tiled run's
+ * Executable after its tile shape (elp_<tx>x<ty>x<tz>), and bin/elp_ne_list
+ * prints the matching ne_list lines (efpol's Ne, its time factor / f). */
+double elp_time_factor(int32_t periodic, int32_t tx, int32_t ty, int32_t tz);
+
 /* Integrity check that allocates nothing.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc -- an application that has given
  * the whole device memory to its own pool, a process under a device-memory
@@ -192,17 +205,18 @@ elp_status elp_set_state(elp_ctx* ctx, const uint32_t* words, const uint32_t* re
  * an error (its steps are incomplete), as elp_sync does. */
 elp_status elp_accepted(elp_ctx* ctx, uint64_t* accepted);
 
-/* Bound of the waits inside tiled launches of several steps.  No counterpart
- * in the reference, whose launches take one step each (gpupol2/gpupol_cuda.cu:
- * 129-146).  A tile of step s waits for the tiles of step s - 1 that overlap
- * it; a wait gives up after `polls` polls (0: the default, about a second)
- * and the launch then reports ELP_ERR_STATE at the next synchronising call.
- * The context stays usable: loading a configuration (elp_init_melt, a load
- * call, elp_set_state) clears the report.  hold_tile >= 0 is a test hook:
- * that tile (work-item index) never announces its first step of a launch,
- * so the tiles waiting on it run out of polls -- the failure path is tested
- * without faulting or hanging the GPU.  -1 announces every tile. */
-elp_status elp_debug_waits(elp_ctx* ctx, uint32_t polls, int32_t hold_tile);
+/* Bound of the grid-barrier waits inside tiled launches of several steps.
+ * No counterpart in the reference, whose launches take one step each
+ * (gpupol2/gpupol_cuda.cu:129-146).  Between two steps the CTAs of a launch
+ * meet at a grid barrier; a wait gives up after `polls` polls (0: the
+ * default, about a second), the launch stops there and reports
+ * ELP_ERR_STATE at the next synchronising call.  The context stays usable:
+ * loading a configuration (elp_init_melt, a load call, elp_set_state) clears
+ * the report.  hold_block >= 0 is a test hook: that CTA of each later launch
+ * never arrives at the first barrier, so every wait there runs out of polls
+ * -- the failure path is tested without faulting or hanging the GPU.  -1
+ * lets every CTA arrive. */
+elp_status elp_debug_waits(elp_ctx* ctx, uint32_t polls, int32_t hold_block);
 
 void elp_destroy(elp_ctx* ctx);
 
@@ -265,10 +279,9 @@ const char* elp_last_error(void);
  * one packed arena; melts with the same domain geometry share one kernel
  * launch and a stream, and groups of different shapes run concurrently.
  * Melts run `steps_per_launch` steps per launch: whole-box melts (L <= 32)
- * on chip, tiled melts as one persistent launch whose tiles of consecutive
- * steps wait only for the tiles they overlap (in a batch of more than one
- * group, tiled groups take one step per launch, so that groups keep
- * overlapping); tiled launches are
+ * on chip, tiled melts as one cooperative launch whose CTAs meet at a grid
+ * barrier between steps (in a batch of more than one group, tiled groups take
+ * one step per launch, so that groups keep overlapping); tiled launches are
  * replayed from a CUDA graph.  A melt gives the same bits in a batch as alone
  * with the same spec, whatever its steps per launch.
  * The reference has no batched engine; its nearest form is one independent

@@ -240,15 +240,15 @@ extern "C" elp_status elp_accepted(elp_ctx* c, uint64_t* acc)
     return elp_device_errors(error_flags(c), c->stream);
 }
 
-extern "C" elp_status elp_debug_waits(elp_ctx* c, uint32_t polls, int32_t hold_tile)
+extern "C" elp_status elp_debug_waits(elp_ctx* c, uint32_t polls, int32_t hold_block)
 {
     if (!c) return elp_fail(ELP_ERR_ARG, "null context");
-    if (hold_tile < -1 || (c->G.nitems > 0 && hold_tile >= c->G.nitems))
-        return elp_fail(ELP_ERR_ARG, "tile %d not in 0..%d", hold_tile, c->G.nitems - 1);
+    if (hold_block < -1 || (c->G.nitems > 0 && hold_block >= c->G.nitems))
+        return elp_fail(ELP_ERR_ARG, "block %d not in 0..%d", hold_block, c->G.nitems - 1);
     ELP_CUDA_TRY(cudaSetDevice(c->device));
     ELP_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->G.wait_polls = polls;
-    c->G.hold_item1 = hold_tile + 1;
+    c->G.hold_cta1 = hold_block + 1;
     if (c->G.graph) {
         // captured launches carry the old bound: capture again on the next run
         cudaGraphExecDestroy(c->G.graph);

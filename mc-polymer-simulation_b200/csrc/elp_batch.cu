@@ -117,10 +117,10 @@ extern "C" elp_status elp_batch_create(const elp_job_spec* specs, int32_t njobs,
         lat_words += ((size_t)mm.g.L * mm.g.L * mm.g.L + 63) / 64 * 64;
         rec_words += (size_t)mm.P * ELP_REC_WORDS;
     }
-    // A tiled launch of several steps keeps its persistent CTAs on their SMs
-    // until its last step, which would serialise the groups that otherwise
-    // overlap.  With more than one group, tiled groups take one step per
-    // launch (the same bits).
+    // A tiled launch of several steps is cooperative: it starts only when all
+    // its CTAs fit at once and then holds every SM until its last step, which
+    // would serialise the groups that otherwise overlap.  With more than one
+    // group, tiled groups take one step per launch (the same bits).
     if (gdesc.size() > 1)
         for (auto& gd : gdesc)
             if (!std::get<0>(gd).periodic) std::get<1>(gd) = 1;

@@ -121,8 +121,8 @@ elp_status elp_device_errors(const uint32_t* d_flags, cudaStream_t s)
         return elp_fail(ELP_ERR_STATE, "a domain held more monomer-0 runs than its label table; steps after the "
                                        "overflow are incomplete (use the generic kernel for this melt)");
     if (flags & 4u)
-        return elp_fail(ELP_ERR_STATE, "a tile gave up waiting for the tiles of the previous step; steps after it "
-                                       "are incomplete");
+        return elp_fail(ELP_ERR_STATE, "a tiled launch of several steps gave up waiting at its grid barrier; steps "
+                                       "after it are incomplete");
     return ELP_OK;
 }
 

@@ -34,11 +34,9 @@ Sweep2Launch make_launch(const elp_group* G, int nsteps, uint32_t step_base, int
     l.args.step_dev = G->d_ctr;
     l.args.table = G->d_table;
     l.args.error = G->d_error;
-    l.args.flow = G->d_ctr + 1;
-    l.args.done = G->d_done;
-    l.args.njobs = (int)G->jobs.size();
+    l.args.grid_bar = G->d_ctr + 1;
     l.args.wait_polls = G->wait_polls;
-    l.args.hold_item1 = G->hold_item1;
+    l.args.hold_cta1 = G->hold_cta1;
     return l;
 }
 
@@ -94,7 +92,7 @@ cudaError_t elp_group_init(elp_group* G, const elp_geometry& geom, int nsm, int 
     G->stream = stream;
     G->d_table = d_table;
     G->d_error = d_error;
-    // step counter and the ticket and exit counts of tiled launches,
+    // step counter and the two counts of the grid barrier of tiled launches,
     // stream-ordered (a group created while others run does not stall them)
     cudaError_t e = cudaMallocAsync((void**)&G->d_ctr, 4 * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
@@ -139,14 +137,10 @@ cudaError_t elp_group_commit(elp_group* G)
     }
     if (nj * nd > G->cap_items) {
         if (G->d_items && (e = cudaFreeAsync(G->d_items, G->stream)) != cudaSuccess) return e;
-        if (G->d_done && (e = cudaFreeAsync(G->d_done, G->stream)) != cudaSuccess) return e;
         G->d_items = nullptr;
-        G->d_done = nullptr;
         G->cap_items = 0;
         const size_t cap = nj * nd < 64 ? 64 : 2 * nj * nd;
         if ((e = cudaMallocAsync((void**)&G->d_items, cap * sizeof(uint2), G->stream)) != cudaSuccess) return e;
-        if ((e = cudaMallocAsync((void**)&G->d_done, cap * sizeof(uint32_t), G->stream)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(G->d_done, 0, cap * sizeof(uint32_t), G->stream)) != cudaSuccess) return e;
         G->cap_items = cap;
     }
     std::vector<uint2> items(nj * nd);
@@ -199,8 +193,8 @@ cudaError_t elp_group_run(elp_group* G, int64_t nsteps)
         }
         return cudaSuccess;
     }
-    // tiled domains: the specialised kernel takes spl steps per launch, the
-    // generic one a single step
+    // tiled domains: the specialised kernel takes spl steps per (cooperative)
+    // launch, the generic one a single step
     const int k = G->specialised ? G->spl : 1;
     const int gsteps = G->graph_steps > k ? G->graph_steps / k * k : k;
     if (G->specialised && G->use_graph && nsteps >= gsteps) {
@@ -243,11 +237,9 @@ void elp_group_free(elp_group* G)
     if (G->stream) cudaStreamSynchronize(G->stream);
     cudaFree(G->d_jobs);
     cudaFree(G->d_items);
-    cudaFree(G->d_done);
     cudaFree(G->d_ctr);
     G->graph = nullptr;
     G->d_jobs = nullptr;
     G->d_items = nullptr;
-    G->d_done = nullptr;
     G->d_ctr = nullptr;
 }

@@ -32,12 +32,11 @@ struct elp_group {
     std::vector<int> N;               // ring length per melt
     BatchJob* d_jobs = nullptr;
     uint2* d_items = nullptr;
-    uint32_t* d_done = nullptr;       // completion flag per work item (tiled dataflow), zero between launches
     int nitems = 0;
     size_t cap_jobs = 0, cap_items = 0;   // grow-only device capacity of the two tables
-    uint32_t* d_ctr = nullptr;        // device step counter, then the ticket and exit counts of tiled launches
-    uint32_t wait_polls = 0;          // bound of the kernel's dependency waits (0: the kernel's default)
-    int hold_item1 = 0;               // test hook: item + 1 that never announces its first step
+    uint32_t* d_ctr = nullptr;        // device step counter, then the grid barrier's two counts
+    uint32_t wait_polls = 0;          // bound of the grid barrier's waits (0: the kernel's default)
+    int hold_cta1 = 0;                // test hook: CTA + 1 that never arrives at the first barrier
     uint64_t steps_done = 0;          // steps since the job table's step0 values
     uint32_t ctr_mirror = 0;          // host copy of *d_ctr
 

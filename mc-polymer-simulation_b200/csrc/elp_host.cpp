@@ -234,6 +234,26 @@ void elp_build_table(uint8_t tab[4096])
     for (int i = 0; i < 4096; i++) tab[i] = (uint8_t)(T.e[i] & 0xff);
 }
 
+// Time factors of tiled geometries, measured against reference efpol
+// ensembles (tests/test_gpu_stats.py); shapes not listed are not measured.
+namespace {
+struct TimeFactor {
+    int tx, ty, tz;
+    double f;
+};
+const TimeFactor kTimeFactors[] = {
+    {0, 0, 0, 0.0},
+};
+}  // namespace
+
+extern "C" double elp_time_factor(int32_t periodic, int32_t tx, int32_t ty, int32_t tz)
+{
+    if (periodic) return 1.0;
+    for (const TimeFactor& t : kTimeFactors)
+        if (t.tx == tx && t.ty == ty && t.tz == tz) return t.f;
+    return 0.0;
+}
+
 // GetNPol, cpupol/efpol_lib.c:50-56
 int elp_get_npol(double density, int N, long sites)
 {

@@ -51,15 +51,10 @@ struct BatchLaunch {
     const uint32_t* step_dev;      // ... and, if set, this device counter (graph replays)
     const uint32_t* table;         // 4096-byte transition table
     uint32_t* error;               // device error flags (bit 0: label slot table overflow,
-                                   // bit 2: a tile's wait for the previous step gave up)
-    // tiled domains: the launch's work items are (step, item) pairs taken in
-    // step order from a ticket counter; a tile waits for the tiles of the
-    // previous step that overlap it on their completion flags
-    uint32_t* flow;                // {ticket, exits}, zero between launches
-    uint32_t* done;                // [nitems] last step (launch-relative, + 1) of each item; zero between launches
-    int njobs;                     // melts in the job table; item index = domain * njobs + melt
-    uint32_t wait_polls;           // polls before a dependency wait gives up (0: about a second)
-    int hold_item1;                // test hook: item + 1 whose first step is never announced (0: none)
+                                   // bit 2: a grid barrier wait gave up)
+    uint32_t* grid_bar;            // tiled domains, nsteps > 1: {arrivals, exits}, zero between launches
+    uint32_t wait_polls;           // polls before a grid barrier wait gives up (0: about a second)
+    int hold_cta1;                 // test hook: CTA + 1 that never arrives at the first barrier (0: none)
 };
 
 #include "elp_internal.h"

@@ -291,8 +291,8 @@ static SGroup* group_for(elp_server* s, SJob* j)
         return nullptr;
     // membership changes every few ticks: a captured graph would be rebuilt
     // about as often as it is replayed, so tiled groups launch directly, one
-    // step per launch (a launch of several tiled steps keeps its persistent
-    // CTAs on every SM it uses until its last step, stalling the other groups)
+    // step per launch (a launch of several tiled steps is cooperative and
+    // holds every SM it uses until its last step, stalling the other groups)
     gp->G.use_graph = 0;
     if (!j->g.periodic) gp->G.spl = 1;
     s->groups.push_back(std::move(gp));

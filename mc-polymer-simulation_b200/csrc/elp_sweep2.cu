@@ -3,13 +3,9 @@
 // Same schedule and results as the generic sweep_kernel (elp_sweep.cu); what
 // changes is how the work is fed to the SM:
 //   * tile edges and shared-memory strides are compile-time constants;
-//   * a ring substep runs in two phases.  Phase 1 reads, for every anchor,
-//     the words the move depends on (anchor, next run, target) and decides
-//     acceptance without storing anything.  The warp's accepted moves are
-//     queued in shared memory (one word each), and phase 2 commits them with
-//     the warp's lanes taking queue entries in order: the new words, the
-//     bookkeeping of monomer 0 and the stores run once per accepted move
-//     instead of once per anchor;
+//   * the K anchors a thread owns in a substep are processed stage by stage
+//     (all first loads, then all second loads, ...), so the dependent
+//     shared-memory loads of independent moves overlap;
 //   * monomer 0's runs are handled inline: while a tile is on chip each
 //     labelled word carries its run length (bits 16-31) and a slot number
 //     (bits 5-15) into a small shared-memory table {chain, offset | site};
@@ -27,11 +23,8 @@
 //     the ragged ends).  Rows are 16-byte aligned in shared memory, and the
 //     threads of a warp take anchors from an 8 x 4 block of rows so that
 //     their first loads hit 32 different banks;
-//   * tiled melts are scheduled as a dataflow over (step, tile) items: CTAs
-//     take items from a ticket counter in step order, and a tile of step s
-//     waits only for the (at most 8) tiles of step s - 1 that overlap it, on
-//     per-tile completion flags.  No CTA waits for the whole grid, and the
-//     tiles of consecutive steps overlap in time.
+//   * the grid is persistent over the tiles, and a launch of several steps
+//     over a tiled box is cooperative, with a grid barrier between steps.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -60,13 +53,40 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p)
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
-}
-// Polls of a dependency flag before a wait gives up (about a second with the
+// Polls of the grid barrier before a wait gives up (about a second with the
 // back-off below); a launch can ask for fewer (BatchLaunch.wait_polls).
 constexpr uint32_t WAIT_POLLS = 1u << 24;
+
+// Barrier over all CTAs of a cooperative launch: each CTA adds one to
+// bar[0] and waits (bounded) until it reaches `target`.  The CTA's stores
+// before it are visible to every CTA's loads after it (tiles are fetched
+// with cp.async.cg and records with ld.global.cg, both through L2).
+// Returns false, in every thread of the CTA, when the wait gave up.
+// `arrive` false (a test) makes the CTA wait without adding its count.
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t target, uint32_t polls, bool arrive)
+{
+    bool ok = true;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (arrive) atomicAdd(bar, 1u);
+        for (uint32_t n = 0; ld_acquire_gpu(bar) < target; n++) {
+            if (n >= polls) { ok = false; break; }
+            __nanosleep(64);
+        }
+    }
+    return __syncthreads_or(!ok) == 0;
+}
+// Last act of every CTA of a cooperative launch: the last one to leave
+// zeroes the barrier counts for the next launch on the stream.
+__device__ __forceinline__ void grid_exit(uint32_t* bar)
+{
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(bar + 1, 1u) == gridDim.x - 1) {
+        atomicExch(bar, 0u);
+        atomicExch(bar + 1, 0u);
+    }
+}
 
 template <int TX, int TY, int TZ, bool PER, int NC, int SX, int SXY, int CAP, int K, int MINB>
 struct Shape {
@@ -88,8 +108,8 @@ struct Shape {
     static constexpr int NOFF = PER ? 27 * 16 : 16;
     // shared-memory word offsets: lattice, transition table (4096 bytes),
     // neighbour offsets (bytes, and for tiles in words too), colours, slot
-    // tables, slot count, ticket, head-move rows, per-warp commit queues
-    // (one word per anchor), and the Philox words when threads own < 4 anchors
+    // tables, slot count, head-move rows, and the Philox words when threads
+    // own < 4 anchors
     static constexpr int TABW = WORDS;
     static constexpr int OFFW = TABW + 1024;
     static constexpr int WOFFW = OFFW + NOFF;
@@ -97,10 +117,8 @@ struct Shape {
     static constexpr int SCHW = COLW + 64;
     static constexpr int SSOW = SCHW + CAP;   // {offset of monomer 0 in its run (bits 0-15), site word (16-31)}
     static constexpr int NSLW = SSOW + CAP;
-    static constexpr int TKW = NSLW + 1;
-    static constexpr int HTABW = TKW + 1;     // table rows (0xf, x): moves of a linear chain's monomer 0
-    static constexpr int QW = (HTABW + 64 + 3) & ~3;
-    static constexpr int RNDW = (QW + A + 3) & ~3;
+    static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
+    static constexpr int RNDW = (HTABW + 64 + 3) & ~3;
     static constexpr int NG = 2 * NC / 4;     // substep groups per step
     static constexpr size_t bytes_with(int groups) { return (size_t)(RNDW + (K < 4 ? groups * G * 4 : 0)) * 4; }
     // Philox words of threads that own < 4 anchors: in tiled domains, where
@@ -176,92 +194,6 @@ __device__ __forceinline__ void follow_label(uint32_t* slot_so, int p, int pB, i
     slot_so[slot] = noff | ((uint32_t)((nl == 0 ? p : (nl == 1 ? pB : pY)) >> 2) << 16);
 }
 
-// Phase 2 of a ring substep: commit one accepted move from its queue word
-// (bits 0-17 anchor byte offset, 18-25 table entry dst1 | dst2 << 4, 26 slot,
-// 27-31 boundary class of a periodic box).  The words are read again: the
-// footprints of a substep's anchors are disjoint, so they still hold what
-// phase 1 read.  Store order B, Y, P: when dst1 == 0 the target is P itself
-// and P's store must come last.
-template <bool PER, int OFFW>
-__device__ __forceinline__ void commit_ring(uint32_t* slot_so, uint32_t qe)
-{
-    const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
-    const int p = (int)(qe & 0x3FFFFu);
-    const uint32_t d1 = (qe >> 18) & 15u, d2 = (qe >> 22) & 15u, s = (qe >> 26) & 1u;
-    const int ob = PER ? 16 * (int)(qe >> 27) : 0;
-    const uint32_t wP = SW(p);
-    const int pB = p + offs[ob + (wP & 15)];
-    const int pY = p + offs[ob + d1];
-    const uint32_t wB = SW(pB), wY = SW(pY);
-    uint32_t nP = wP & ~15u;
-    nP = (s == 0) ? nP - ELP_CUNIT : (d1 ? nP : nP + ELP_CUNIT);
-    nP |= d1 ? d1 : d2;
-    uint32_t nB = (wB >= 2u * ELP_CUNIT) ? wB - ELP_CUNIT : 0u;
-    uint32_t nY = d2 ? (d2 | ELP_CUNIT) : wY + ELP_CUNIT;
-    if ((wP | (s ? wB : 0u) | (d2 == 0 ? wY : 0u)) & ELP_LBIT)
-        follow_label(slot_so, p, pB, pY, wP, wB, wY, s, d1, nP, nB, nY);
-    if (s) SW(pB) = nB;
-    if (d1) SW(pY) = nY;
-    SW(p) = nP;
-}
-
-// One ring substep of a thread's K anchors.  Anchor q takes its random byte
-// at bit offset bsh[q] of the Philox word w: bit 0 slot (0: the last monomer
-// of P's run, 1: the first monomer of the next run), bits 1-4 table option.
-// Returns the warp's accepted moves (the same value in every lane).
-template <int K, bool PER, int NC, int TABW, int OFFW>
-__device__ __forceinline__ uint32_t substep_ring(uint32_t* slot_so, uint32_t* queue, const int (&base4)[K],
-                                                 const int (&rot4)[K], const int (&clsyz)[K], const int (&xj4)[K],
-                                                 const int (&bsh)[K], int c4, uint32_t w, int L)
-{
-    const uint8_t* tab = reinterpret_cast<const uint8_t*>(g_smem + TABW);
-    const int* offs = reinterpret_cast<const int*>(g_smem + OFFW);
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t below = (1u << lane) - 1u;
-    uint32_t n = 0;
-#pragma unroll
-    for (int q = 0; q < K; q++) {
-        int xr4 = c4 + rot4[q];
-        if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
-        else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
-        const int p = base4[q] + xr4;
-        int cls = 0;
-        if (PER) {
-            const int x4 = xr4 + xj4[q];
-            cls = clsyz[q] + (x4 == 0 ? 0 : (x4 == 4 * (L - 1) ? 2 : 1));
-        }
-        const int ob = 16 * cls;
-        const uint32_t wP = SW(p);
-        const uint32_t rb = w >> bsh[q];
-        const uint32_t bo = wP & 15;
-        // the next run's word: inside the anchor's radius-1 ball, which no
-        // other anchor of this substep touches (an empty P reads itself)
-        const uint32_t wB = SW(p + offs[ob + bo]);
-        // source bonds (b_{m-1}, b_m): slot 0 uses row (0, b_out(P)) when P's
-        // run holds two or more, else row (0, 0); slot 1 uses row (b_out(P),
-        // next run > 1 ? 0 : b_out(next)).  Rows (0, 0) and (x, 3) hold only
-        // null moves, which covers an empty P, a run of one in slot 0 and a
-        // next run in the halo.
-        const uint32_t s = rb & 1u;
-        const uint32_t v = s ? wB : wP;
-        const bool many = v >= 2u * ELP_CUNIT;
-        const uint32_t src2 = (many != (s != 0)) ? (v & 15u) : 0u;
-        const uint32_t e = tab[((s ? bo : 0u) << 8) | (src2 << 4) | ((rb >> 1) & 15u)];
-        const uint32_t d1 = e & 15u;
-        const uint32_t wY = SW(p + offs[ob + d1]);
-        // accept: the monomer joins the next run (dst2 == 0, which must not
-        // be the halo) or moves to a free site or stays on P (dst1 == 0)
-        const bool ok = e != 0 && ((e >> 4) == 0 ? wY != HWALL : (d1 == 0 || wY == 0));
-        const uint32_t bal = __ballot_sync(0xffffffffu, ok);
-        if (ok) queue[n + __popc(bal & below)] = (uint32_t)p | (e << 18) | (s << 26) | ((uint32_t)cls << 27);
-        n += __popc(bal);
-    }
-    __syncwarp();
-    for (uint32_t b = 0; b < n; b += 32)
-        if (b + lane < n) commit_ring<PER, OFFW>(slot_so, queue[b + lane]);
-    return n;
-}
-
 // One substep of a thread's K anchors with the general move (op: words in
 // their global form, monomer 0's bookkeeping in the chain records, halo
 // words ELP_WALL), for a ring tile whose monomer-0 runs outnumber the slots.
@@ -281,12 +213,14 @@ __device__ __forceinline__ uint32_t substep_general(const Dom& D, const int (&ba
     return acc;
 }
 
-// The K anchors of one thread, one substep, for melts that may hold linear
-// chains (one phase, with the head moves of monomer 0).  Returns accepted
-// moves.  Byte offsets: anchors base4 + 4 xr, colour c4 = 4 c, neighbour
-// offsets at OFFW words; transition table (bytes) at TABW words.
+// The K anchors of one thread, one substep.  Returns accepted moves.  Anchor
+// q takes its random byte at bit offset bsh[q] of the Philox word w: bit 0
+// slot (0: the last monomer of P's run, 1: the first monomer of the next
+// run), bits 1-4 table option.  Byte offsets: anchors base4 + 4 xr, colour
+// c4 = 4 c, neighbour offsets at OFFW words; transition table (bytes) at
+// TABW words.  `lin`: the melt holds linear chains (head moves of monomer 0).
 template <int K, bool PER, int NC, int TABW, int OFFW, int HTABW>
-__device__ __forceinline__ int substep_lin(uint32_t* slot_so, const int (&base4)[K], const int (&rot4)[K],
+__device__ __forceinline__ int substepK(uint32_t* slot_so, const int (&base4)[K], const int (&rot4)[K],
                                            const int (&clsyz)[K], const int (&xj4)[K], const int (&bsh)[K],
                                            const int (&an)[K], int c4, uint32_t w, int L, bool lin, uint32_t t, int d,
                                            int k, uint2 key)
@@ -414,8 +348,6 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     uint32_t* slot_chain = g_smem + SH::SCHW;
     uint32_t* slot_so = g_smem + SH::SSOW;
     uint32_t* nslots = g_smem + SH::NSLW;
-    uint32_t* ticket = g_smem + SH::TKW;
-    uint32_t* queue = g_smem + SH::QW + (threadIdx.x >> 5) * 32 * K;
     uint4* rnd = reinterpret_cast<uint4*>(g_smem + SH::RNDW);
     const int tid = threadIdx.x;
     const int cx = tid % TX;  // the tile column this thread loads, scans and stores
@@ -479,27 +411,22 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     }
     const uint32_t step_dev = a.step_dev ? *a.step_dev : 0u;
     const uint32_t polls = a.wait_polls ? a.wait_polls : WAIT_POLLS;
-    // Whole-box domains run their steps back to back on chip, one work item
-    // per melt.  Tiled domains move their tiles every step: the work items
-    // are (step, tile) pairs, taken in step order from a ticket counter.
-    const int inner = PER ? a.nsteps : 1;
-    const uint32_t total = PER ? (uint32_t)a.nitems : (uint32_t)a.nitems * (uint32_t)a.nsteps;
-    uint32_t next = blockIdx.x;
+    // Whole-box domains run their steps back to back on chip; tiled domains
+    // move their tiles every step, so a launch of several steps takes its
+    // steps one after another over all tiles, with a grid barrier between
+    // steps (the launch is cooperative: all CTAs are resident).
+    const int outer = PER ? 1 : a.nsteps, inner = PER ? a.nsteps : 1;
 
-    for (;;) {
-        uint32_t tk;
-        if (PER) {
-            tk = next;
-            next += gridDim.x;
-        } else {
-            __syncthreads();   // the previous item is done with the ticket word
-            if (tid == 0) *ticket = atomicAdd(a.flow, 1u);
-            __syncthreads();
-            tk = *ticket;
+    for (int so = 0; so < outer; so++) {
+    if (so > 0) {
+        // a test may keep one CTA from arriving at the first barrier
+        const bool arrive = !(so == 1 && (int)blockIdx.x + 1 == a.hold_cta1);
+        if (!grid_barrier(a.grid_bar, gridDim.x * (uint32_t)so, polls, arrive)) {
+            if (tid == 0) atomicOr(a.error, 4u);
+            break;
         }
-        if (tk >= total) break;
-        const int so = PER ? 0 : (int)(tk / (uint32_t)a.nitems);
-        const int it = PER ? (int)tk : (int)(tk % (uint32_t)a.nitems);
+    }
+    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
         const uint2 item = a.items[it];
         const BatchJob& J = a.jobs[item.x];
         const int d = (int)item.y;
@@ -515,50 +442,12 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
         D.ox = SH::OX; D.sx = SX; D.sxy = SXY; D.L = L;
         D.x0 = 0; D.y0 = 0; D.z0 = 0;
         uint32_t accepted = 0;
-        bool overflow = false, skip = false, spill = false;
+        bool overflow = false, spill = false;
         int bse[K];   // anchor base byte offsets of this tile (plus its offset sh in the spans)
 #pragma unroll
         for (int q = 0; q < K; q++) bse[q] = base[q];
 
-        if constexpr (!PER) if (so > 0) {
-            // wait for the tiles of the previous step that overlap this one:
-            // per axis the tile with the same index and, when the origin
-            // moved, the neighbour on the side it moved to (threads 0-7 each
-            // take one of the 2 x 2 x 2 combinations)
-            bool ok = true;
-            if (tid < 8) {
-                const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)so;
-                const uint4 sc = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
-                const uint4 sp = philox(make_uint4(t - 1u, 0, ELP_STREAM_SHIFT, 0), key);
-                const int ci = d % ntx, cj = (d / ntx) % nty, ck = d / ntx / nty;
-                const int ntz = J.ntz;
-                int ii = ci, jj = cj, kk = ck;
-                const int ax = (int)bounded(sc.x, TX), px = (int)bounded(sp.x, TX);
-                const int ay = (int)bounded(sc.y, TY), py = (int)bounded(sp.y, TY);
-                const int az = (int)bounded(sc.z, TZ), pz = (int)bounded(sp.z, TZ);
-                ii += (tid & 1) ? (ax > px ? 1 : 0) : (ax < px ? -1 : 0);
-                jj += (tid & 2) ? (ay > py ? 1 : 0) : (ay < py ? -1 : 0);
-                kk += (tid & 4) ? (az > pz ? 1 : 0) : (az < pz ? -1 : 0);
-                ii += ii < 0 ? ntx : 0; ii -= ii >= ntx ? ntx : 0;
-                jj += jj < 0 ? nty : 0; jj -= jj >= nty ? nty : 0;
-                kk += kk < 0 ? ntz : 0; kk -= kk >= ntz ? ntz : 0;
-                const uint32_t* f = a.done + (size_t)(ii + ntx * (jj + nty * kk)) * a.njobs + item.x;
-                const uint32_t need = (uint32_t)so;   // the previous step announced as so
-                for (uint32_t n = 0; ld_acquire_gpu(f) < need; n++) {
-                    if (n >= polls) { ok = false; break; }
-                    __nanosleep(32);
-                }
-            }
-            if (__syncthreads_or(!ok)) {
-                // a dependency did not finish in time: leave this tile as it
-                // is (its words are not read while they may be written) and
-                // report; the flag below still lets later tiles proceed
-                if (tid == 0) atomicOr(a.error, 4u);
-                skip = true;
-            }
-        }
-
-        for (int st = 0; st < inner && !overflow && !skip; st++) {
+        for (int st = 0; st < inner && !overflow; st++) {
             const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)(so + st);
             if (!PER) {
                 const uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
@@ -706,15 +595,10 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                 for (int kk = 0; kk < 4; kk++) {
                     if (!PER && spill)
                         accepted += substep_general<K, NC, SH::WOFFW>(D, bse, rot, bsh, (int)col[k + kk], rws[kk]);
-                    else if (LIN)
-                        accepted += (uint32_t)substep_lin<K, PER, NC, TABW, OFFW, HTABW>(
+                    else
+                        accepted += (uint32_t)substepK<K, PER, NC, TABW, OFFW, HTABW>(
                             slot_so, bse, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d, k + kk,
                             key);
-                    else {
-                        const uint32_t n = substep_ring<K, PER, NC, TABW, OFFW>(
-                            slot_so, queue, bse, rot, clsyz, xj, bsh, (int)col[k + kk], rws[kk], LP);
-                        accepted += (tid & 31) == 0 ? n : 0u;
-                    }
                     __syncthreads();
                 }
             }
@@ -724,7 +608,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             for (int i = tid; i < SH::WORDS; i += THREADS)
                 if (S[i] == ELP_WALL) S[i] = HWALL;
         }
-        if (!overflow && !skip) {
+        if (!overflow) {
             const uint32_t ns = spill ? 0u : *nslots;   // a spilled tile's records are already written
             for (uint32_t sl = tid; sl < ns; sl += THREADS) {
                 const uint32_t so16 = slot_so[sl];
@@ -770,39 +654,17 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if ((tid & 31) == 0 && v) atomicAdd(J.acc, v);
         }
-        if (!PER) {
-            // announce the tile's step: its stores (lattice and records) are
-            // visible to every CTA that sees the flag (release after the CTA
-            // barrier; readers acquire, then barrier, then load through L2).
-            // A test may hold back one item's first announcement.
-            __syncthreads();
-            if (tid == 0 && !(so == 0 && it + 1 == a.hold_item1)) {
-                __threadfence();
-                st_release_gpu(a.done + it, (uint32_t)so + 1u);
-            }
-        }
     }
-    if (!PER) {
-        // the last CTA out clears the flags and the ticket for the next launch
-        __syncthreads();
-        bool last = false;
-        if (tid == 0) last = atomicAdd(a.flow + 1, 1u) == gridDim.x - 1;
-        if (__syncthreads_or(last)) {
-            for (int i = tid; i < a.nitems; i += THREADS) a.done[i] = 0u;
-            if (tid == 0) {
-                a.flow[0] = 0u;
-                a.flow[1] = 0u;
-            }
-        }
     }
+    if (!PER && a.nsteps > 1) grid_exit(a.grid_bar);
 }
 
 }  // namespace elp
 
 // ---- dispatch ----------------------------------------------------------------
 namespace {
-// Resident CTAs per SM of one kernel, per device (the launch sizes the
-// persistent grid by it); 0 until the first launch on that device asks.
+// Resident CTAs per SM of one kernel, per device (a cooperative launch is
+// sized by it); 0 until the group set-up on that device has asked.
 constexpr int MAX_DEVICES = 64;
 }
 
@@ -835,15 +697,30 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
         const_cast<Sweep2Launch*>(l)->smem_out = SH::BYTES;
         return cudaSuccess;
     }
-    const int resident = l->nsm * (per_sm[dev].load() > 0 ? per_sm[dev].load() : MINB);
-    long work = l->args.nitems;
-    if (!PER) work *= (l->args.nsteps > 0 ? l->args.nsteps : 1);
-    int grid = (int)(work < resident ? work : resident);
+    int grid = l->args.nitems;
+    if (PER || l->args.nsteps <= 1) {
+        if (grid > l->nsm * MINB) grid = l->nsm * MINB;
+        if (grid < 1) return cudaSuccess;
+        k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
+        return cudaGetLastError();
+    }
+    // tiled, several steps: a cooperative launch (every CTA resident, or an
+    // error) of at most as many CTAs as fit on the device at once
+    const int per = per_sm[dev].load();
+    if (per < 1) return cudaErrorNotSupported;
+    if (grid > l->nsm * per) grid = l->nsm * per;
     if (grid < 1) return cudaSuccess;
-    // tiled launches need no co-residency: a CTA only ever waits for items
-    // with smaller tickets, which CTAs already running hold
-    k<<<grid, THREADS, SH::BYTES, s>>>(l->args);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SH::BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, l->args);
 }
 
 // Launch (or, with check_only, test) the specialised kernel for a shape.
@@ -852,7 +729,7 @@ static cudaError_t launch2(const Sweep2Launch* l, cudaStream_t s)
 extern "C" cudaError_t elp_launch_sweep2(const Sweep2Launch* l, cudaStream_t s)
 {
     const elp_geometry& g = l->geom;
-    if (!g.periodic && (!l->args.flow || !l->args.done)) return cudaErrorNotSupported;
+    if (l->args.nsteps > 1 && !g.periodic && !l->args.grid_bar) return cudaErrorNotSupported;
 // shape: tile edges, whole box or tiled, colour modulus, shared-memory
 // strides, slot capacity, anchors per thread, threads, min blocks per SM
 #define SHAPE(X_, Y_, Z_, PER_, NC_, SX_, SXY_, CAP_, K_, THR_, MINB_)                                        \

@@ -41,7 +41,7 @@ class Info(C.Structure):
 EXPORTED = [
     "elp_default_spec", "elp_create", "elp_init_melt", "elp_load_chains", "elp_load_tuv", "elp_run",
     "elp_run_timed", "elp_stream", "elp_sync", "elp_fetch_chains", "elp_fetch_checked", "elp_write_tuv", "elp_check", "elp_get_info",
-    "elp_get_state", "elp_set_state", "elp_accepted", "elp_debug_waits", "elp_destroy", "elp_transition_table",
+    "elp_get_state", "elp_set_state", "elp_accepted", "elp_debug_waits", "elp_time_factor", "elp_destroy", "elp_transition_table",
     "elp_format_tuv", "elp_status_string", "elp_last_error",
     "elp_batch_create", "elp_batch_size", "elp_batch_init_melts", "elp_batch_load_chains", "elp_batch_run",
     "elp_batch_run_timed", "elp_batch_sync", "elp_batch_fetch_chains", "elp_batch_get_state", "elp_batch_check",
@@ -84,6 +84,7 @@ def lib():
         "elp_set_state": (i32, [vp, vp, vp, u64]),
         "elp_accepted": (i32, [vp, vp]),
         "elp_debug_waits": (i32, [vp, u32, i32]),
+        "elp_time_factor": (C.c_double, [i32, i32, i32, i32]),
         "elp_destroy": (None, [vp]),
         "elp_transition_table": (i32, [vp]),
         "elp_format_tuv": (i32, [i32, i32, i32, vp, vp, vp, C.c_size_t, vp]),
@@ -138,6 +139,12 @@ def transition_table() -> np.ndarray:
     out = np.zeros(4096, dtype=np.uint8)
     check(lib().elp_transition_table(out.ctypes.data))
     return out
+
+
+def time_factor(periodic, tx, ty, tz) -> float:
+    """Clock of a domain geometry against reference efpol's (elp_time_factor);
+    0 for a tile shape not measured."""
+    return lib().elp_time_factor(int(periodic), tx, ty, tz)
 
 
 def format_tuv(L, start, bonds) -> str:
@@ -310,9 +317,9 @@ class Melt:
         check(lib().elp_accepted(self.h, C.byref(v)))
         return v.value
 
-    def debug_waits(self, polls=0, hold_tile=-1):
-        """Bound of the waits in tiled multi-step launches (elp_debug_waits)."""
-        check(lib().elp_debug_waits(self.h, polls, hold_tile))
+    def debug_waits(self, polls=0, hold_block=-1):
+        """Bound of the grid-barrier waits in tiled multi-step launches (elp_debug_waits)."""
+        check(lib().elp_debug_waits(self.h, polls, hold_block))
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

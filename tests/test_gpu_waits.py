@@ -1,13 +1,11 @@
-"""The bounded waits of tiled launches of several steps.
+"""The bounded grid-barrier waits of tiled launches of several steps.
 
-Inside one launch a tile of step s waits for the tiles of step s - 1 that
-overlap it (per-tile completion flags, no grid-wide barrier).  Every wait is
-bounded: when it runs out, the tile is left as it is, the launch reports
+Between two steps the CTAs of a cooperative launch meet at a grid barrier.
+Every wait there is bounded: when it runs out, the launch stops, reports
 through the device error flags, and the next synchronising call returns
-ELP_ERR_STATE.  These tests make a wait run out on purpose, without any GPU
-fault: one tile is told never to announce its first step (elp_debug_waits),
-so the tiles that overlap it in the second step poll a flag that nothing
-sets until their short limit is reached.
+ELP_ERR_STATE.  This test makes the wait run out on purpose, without any GPU
+fault: one CTA is told never to arrive (elp_debug_waits), so every CTA polls
+a count that never reaches its target until a short limit is reached.
 """
 import numpy as np
 import pytest
@@ -23,12 +21,12 @@ def test_a_wait_that_runs_out_reports_and_leaves_the_context_usable():
     m.init_melt()
     m.run(8)
     m.sync()                                     # normal launches: no report
-    m.debug_waits(polls=2000, hold_tile=0)
+    m.debug_waits(polls=2000, hold_block=0)
     m.run(4)
     with pytest.raises(elp.ElpError) as e:
         m.sync()
     assert e.value.status == elp.ERR_STATE
-    assert "previous step" in str(e.value)
+    assert "grid barrier" in str(e.value)
     with pytest.raises(elp.ElpError):
         m.accepted()                             # the count of incomplete steps is flagged too
     # a new configuration clears the report; the trajectory is the normal one
@@ -44,8 +42,8 @@ def test_a_wait_that_runs_out_reports_and_leaves_the_context_usable():
     assert m.check() == 0
 
 
-def test_bad_tile_index_is_an_argument_error():
+def test_bad_block_index_is_an_argument_error():
     m = elp.Melt(seed=5, **GEOM)
     with pytest.raises(elp.ElpError) as e:
-        m.debug_waits(10, 8)                     # 8 tiles: 0..7
+        m.debug_waits(10, 8)                     # 8 tiles, 8 CTAs: 0..7
     assert e.value.status == elp.ERR_ARG
