@@ -194,21 +194,57 @@ __device__ __forceinline__ void follow_label(uint32_t* slot_so, int p, int pB, i
     slot_so[slot] = noff | ((uint32_t)((nl == 0 ? p : (nl == 1 ? pB : pY)) >> 2) << 16);
 }
 
-// One substep of a thread's K anchors with the general move (op: words in
-// their global form, monomer 0's bookkeeping in the chain records, halo
-// words ELP_WALL), for a ring tile whose monomer-0 runs outnumber the slots.
-template <int K, int NC, int WOFFW>
-__device__ __forceinline__ uint32_t substep_general(const Dom& D, const int (&base4)[K], const int (&rot4)[K],
-                                                    const int (&bsh)[K], int c4, uint32_t w)
+// The Philox word of substep group k / 4 for this thread's anchors (counter
+// word 3 gq).  Threads owning four anchors draw it themselves; with PRE all
+// of the step's words were drawn while the tile loaded; otherwise G threads
+// draw the next group's words into the other of two buffers while this group
+// runs (read four barriers ago).
+template <int K, bool PRE, int G, int NSUB>
+__device__ __forceinline__ uint4 group_words(uint4* rnd, int k, uint32_t t, int d, int gq, uint2 key)
 {
+    if (K == 4) return philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)gq), key);
+    if (PRE) return rnd[(k >> 2) * G + gq];
+    const int cur = (k >> 2) & 1;
+    const uint4 rw = rnd[cur * G + gq];
+    if ((int)threadIdx.x < G && k + 4 < NSUB)
+        rnd[(cur ^ 1) * G + threadIdx.x] = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2) + 1u, threadIdx.x), key);
+    return rw;
+}
+
+// All substeps of a ring tile whose monomer-0 runs outnumber the slots, with
+// the general move (op: words in their global form, monomer 0's bookkeeping
+// in the chain records, halo words ELP_WALL).  Not inlined: it runs rarely,
+// and its registers stay out of the main substep loop.  Same anchors, random
+// words and order as the main loop.  Returns this thread's accepted moves.
+// This thread's anchors, passed by value so that the caller's copies stay in
+// registers.
+template <int K>
+struct AnchorSet {
+    int bse[K], rot[K], bsh[K];
+};
+
+template <int K, int NC, int WOFFW, bool PRE, int G>
+__device__ __noinline__ uint32_t general_substeps(const Dom D, const AnchorSet<K> an, const uint32_t* col, uint4* rnd,
+                                                  uint32_t t, int d, int gq, uint2 key)
+{
+    const int* bse = an.bse;
+    const int* rot = an.rot;
+    const int* bsh = an.bsh;
     const int* woffs = reinterpret_cast<const int*>(g_smem + WOFFW);
     uint32_t acc = 0;
-#pragma unroll
-    for (int q = 0; q < K; q++) {
-        int xr4 = c4 + rot4[q];
-        if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
-        else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
-        acc += (uint32_t)op(D, (base4[q] + xr4) >> 2, woffs, (w >> bsh[q]) & 0xffu);
+    for (int k = 0; k < 2 * NC; k += 4) {
+        const uint4 rw = group_words<K, PRE, G, 2 * NC>(rnd, k, t, d, gq, key);
+        const uint32_t rws[4] = {rw.x, rw.y, rw.z, rw.w};
+        for (int kk = 0; kk < 4; kk++) {
+            const int c4 = (int)col[k + kk];
+            for (int q = 0; q < K; q++) {
+                int xr4 = c4 + rot[q];
+                if ((NC & (NC - 1)) == 0) xr4 &= 4 * (NC - 1);
+                else xr4 -= xr4 >= 4 * NC ? 4 * NC : 0;
+                acc += (uint32_t)op(D, (bse[q] + xr4) >> 2, woffs, (rws[kk] >> bsh[q]) & 0xffu);
+            }
+            __syncthreads();
+        }
     }
     return acc;
 }
@@ -573,32 +609,25 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
                     if (S[i] == HWALL) S[i] = ELP_WALL;
                 __syncthreads();
             }
+            if (!PER && spill) {
+                AnchorSet<K> as;
+#pragma unroll
+                for (int q = 0; q < K; q++) {
+                    as.bse[q] = bse[q];
+                    as.rot[q] = rot[q];
+                    as.bsh[q] = bsh[q];
+                }
+                accepted += general_substeps<K, NC, SH::WOFFW, SH::PRE, SH::G>(D, as, col, rnd, t, d, gq, key);
+                continue;
+            }
 #pragma unroll 1
             for (int k = 0; k < 2 * NC; k += 4) {
-                uint4 rw;
-                if (K == 4) {
-                    rw = philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2), (uint32_t)gq), key);
-                } else if (SH::PRE) {
-                    rw = rnd[(k >> 2) * SH::G + gq];
-                } else {
-                    // this group's words were drawn during the previous one (or
-                    // before the first); G threads now draw the next group's
-                    // into the other buffer, read four barriers ago
-                    const int cur = (k >> 2) & 1;
-                    rw = rnd[cur * SH::G + gq];
-                    if (tid < SH::G && k + 4 < 2 * NC)
-                        rnd[(cur ^ 1) * SH::G + tid] =
-                            philox(make_uint4(t, (uint32_t)d, (uint32_t)(k >> 2) + 1u, (uint32_t)tid), key);
-                }
+                const uint4 rw = group_words<K, SH::PRE, SH::G, 2 * NC>(rnd, k, t, d, gq, key);
                 const uint32_t rws[4] = {rw.x, rw.y, rw.z, rw.w};
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++) {
-                    if (!PER && spill)
-                        accepted += substep_general<K, NC, SH::WOFFW>(D, bse, rot, bsh, (int)col[k + kk], rws[kk]);
-                    else
-                        accepted += (uint32_t)substepK<K, PER, NC, TABW, OFFW, HTABW>(
-                            slot_so, bse, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d, k + kk,
-                            key);
+                    accepted += (uint32_t)substepK<K, PER, NC, TABW, OFFW, HTABW>(
+                        slot_so, bse, rot, clsyz, xj, bsh, anq, (int)col[k + kk], rws[kk], LP, lin, t, d, k + kk, key);
                     __syncthreads();
                 }
             }

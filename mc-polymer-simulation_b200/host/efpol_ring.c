@@ -17,8 +17,11 @@
  * integrity failure, 193 unknown or unsupported model (sl_equal only), 212
  * melt too small to halve.  With ELP_PTL=1 in the environment the per-ring
  * time series DIR/N_<N_i>/ptl/pol=<p>_dev=0.res are written during the run
- * as well.  "Executable = efpol" is written because the dynamics are
- * efpol's single-monomer dynamics (same move table and attempt rate).
+ * as well.  A whole-box level writes "Executable = efpol": its dynamics are
+ * efpol's single-monomer dynamics (same move table and attempt rate).  A
+ * tiled level (L > 32) writes elp_<tx>x<ty>x<tz>, its tile shape: the tile
+ * walls slow its clock by elp_time_factor, and bin/elp_ne_list gives the
+ * analysis the matching time factor.
  */
 #include <errno.h>
 #include <stdio.h>
@@ -219,7 +222,10 @@ int main(int argc, char** argv)
         fprintf(f, "Equilibrated = 0\n");
         fprintf(f, "Npol = %i\n", P);
         fprintf(f, "Polymodel = sl_equal\n");
-        fprintf(f, "Executable = efpol\n");
+        if (info.periodic)
+            fprintf(f, "Executable = efpol\n");
+        else
+            fprintf(f, "Executable = elp_%dx%dx%d\n", info.tile[0], info.tile[1], info.tile[2]);
         fclose(f);
         if ((st = elp_dumper_close(&dumper))) return die(st, 192);
         elp_destroy(ctx);

@@ -13,7 +13,9 @@
  * so it is bit-identical to an uninterrupted run.  The box must be cubic
  * (LT = LU = LV).  The initial melt is the efpol one and the dynamics are
  * efpol's single-monomer dynamics, hence "Executable = efpol" in the
- * settings (the analysis picks its time factor from that name).  With
+ * settings of a whole-box run (the analysis picks its time factor from that
+ * name); a tiled run writes elp_<tx>x<ty>x<tz>, its tile shape, whose
+ * slower clock (elp_time_factor) bin/elp_ne_list gives the analysis.  With
  * ELP_PTL=1 in the environment a fresh run also writes the per-ring time
  * series DIR/ptl/pol=<p>_dev=0.res during the run (not on resume: those files
  * would have to cover the earlier dumps too).
@@ -176,7 +178,10 @@ int main(int argc, char** argv)
     fprintf(f, "Equilibrated = %i\n", equil);
     fprintf(f, "Npol = %i\n", info.P);
     fprintf(f, "Polymodel = sl_equal\n");
-    fprintf(f, "Executable = efpol\n");
+    if (info.periodic)
+        fprintf(f, "Executable = efpol\n");
+    else
+        fprintf(f, "Executable = elp_%dx%dx%d\n", info.tile[0], info.tile[1], info.tile[2]);
     fprintf(f, "Fast_equilibration = %i\n", fasteq ? 1 : 0);
     fprintf(f, "FEQ_timestep = %i\n", fasteq);
     fprintf(f, "Release = elp-b200\n");

@@ -81,3 +81,50 @@ def test_statistics_match_reference_efpol(name, seeds, linear):
         d, se, ma, mg = compare(ref["per_seed"], gpu, key, idx)
         rows.append((key, idx, ma, mg, d, se))
         assert d <= Z * se, f"{key}[{idx}]: efpol {ma:.5g} vs GPU {mg:.5g} differ by {d:.3g} > {Z} x {se:.3g}"
+
+
+# Tiled geometries: L=64 melts run as 32^3 tiles (the default at L=64 and
+# L=256) or 32x16x16 tiles (the default at L=128).  A move whose footprint
+# crosses a tile wall is rejected, as gpupol's out-of-block moves are
+# (gpupol2/ringpol3.cu:58-76); the walls move every step, so the equilibrium
+# (Rg^2, stored length, run lengths) is efpol's, compared here over steps
+# 15000-50000, while the clock runs slower: the GPU's centre-of-mass MSD
+# after t steps is efpol's after f*t steps, f the time factor that
+# elp_time_factor records for the shape (and the drop-in programs hand to
+# the analysis through their Executable name).
+TILED = [((32, 32, 32), range(7001, 7009)), ((32, 16, 16), range(7101, 7109))]
+
+
+def msd_step_ratio(lags, ref_msd, msd):
+    """Per lag, the factor f with msd(lag) = ref_msd(f * lag), ref_msd
+    interpolated (and at the ends extrapolated) linearly in log-log."""
+    x, y = np.log(lags), np.log(ref_msd)
+    out = []
+    for lx, v in zip(x, np.log(msd)):
+        if v <= y[0]:
+            X = x[0] + (v - y[0]) * (x[1] - x[0]) / (y[1] - y[0])
+        elif v >= y[-1]:
+            X = x[-1] + (v - y[-1]) * (x[-1] - x[-2]) / (y[-1] - y[-2])
+        else:
+            X = np.interp(v, y, x)
+        out.append(np.exp(X - lx))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("tile,seeds", TILED)
+def test_tiled_statistics_match_reference_efpol(tile, seeds):
+    ref = json.load(open(os.path.join(GOLD, "efpol_stats_L64_N100.json")))
+    gpu = gpu_ensemble(ref["L"], ref["N"], ref["steps"], ref["interval"], ref["therm"], ref["msd_lags_intervals"],
+                       list(seeds), periodic=0, tile=tile)
+    for key, idx in [("rg2", None), ("sl_frac", None)] + [("run_hist", i) for i in range(4)]:
+        d, se, ma, mg = compare(ref["per_seed"], gpu, key, idx)
+        assert d <= Z * se, f"{tile} {key}[{idx}]: efpol {ma:.5g} vs GPU {mg:.5g} differ by {d:.3g} > {Z} x {se:.3g}"
+    lags = np.array(ref["msd_lags_intervals"], dtype=float)
+    ma = np.mean([s["msd"] for s in ref["per_seed"]], axis=0)
+    per_seed = np.array([msd_step_ratio(lags, ma, s["msd"]) for s in gpu])
+    f = per_seed.mean(axis=0)
+    f_se = per_seed.std(axis=0, ddof=1) / np.sqrt(len(per_seed))
+    rec = elp.time_factor(0, *tile)
+    assert rec > 0
+    # the recorded factor has three decimals: half a unit of the last one is slack
+    assert np.all(np.abs(f - rec) <= Z * f_se + 0.0005), f"{tile}: step ratio per lag {np.round(f, 4)} vs {rec}"
