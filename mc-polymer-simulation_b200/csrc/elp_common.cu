@@ -53,8 +53,16 @@ extern "C" void elp_default_spec(elp_job_spec* s)
     s->steps_per_launch = 1;
 }
 
-// Domain geometry: the whole box on chip when it fits, else the first tile
-// shape of the preference list that divides the box.
+// Domain geometry: the whole box on chip when it fits, else a tile shape.
+// The first choice depends on the box: attempted moves/s times the shape's
+// time factor (the physical rate) was measured for single relaxed melts at
+// L = 48, 64, 96, 128, 192, 256, 320 and 512.  Below L = 128, 16^3 tiles
+// give the most CTAs and win (L = 64: 13.8 against 12.3 for 32x16x16 and
+// 5.5 for 32^3, G moves/s x f); from 128 to 256, 32x16x16 tiles fill the
+// SMs at two CTAs each (L = 256: 118 against 111 for 32^3); above 256, the
+// 32^3 tiles' slower-wall clock wins (L = 512: 128 against 121).  A box
+// that the first choice does not divide takes the first shape of the list
+// that does.
 static int pick_geometry(const elp_job_spec* s, elp_geometry* g)
 {
     const int L = s->L;
@@ -74,11 +82,14 @@ static int pick_geometry(const elp_job_spec* s, elp_geometry* g)
     }
     static const int cand[][3] = {{32, 32, 32}, {48, 24, 24}, {32, 32, 16}, {24, 24, 24}, {32, 16, 16},
                                   {16, 16, 16}, {40, 20, 20}, {20, 20, 20}, {16, 16, 8}};
-    int first = 0;
-    // L = 128: 256 domains of 32x32x16 / 2 at two CTAs per SM rather than 128
-    // of 32x32x16 on 128 of the SMs (more attempted and more accepted moves/s)
-    if (L == 128) first = 4;
-    for (size_t i = (size_t)first; i < sizeof(cand) / sizeof(cand[0]); i++) {
+    const int n = (int)(sizeof(cand) / sizeof(cand[0]));
+    int order[2 + sizeof(cand) / sizeof(cand[0])];
+    int no = 0;
+    if (L < 128) order[no++] = 5;                       // 16^3
+    else if (L <= 256) { order[no++] = 4; order[no++] = 5; }  // 32x16x16, then 16^3
+    for (int i = 0; i < n; i++) order[no++] = i;
+    for (int k = 0; k < no; k++) {
+        const int i = order[k];
         g->tx = cand[i][0]; g->ty = cand[i][1]; g->tz = cand[i][2];
         if (L % g->tx || L % g->ty || L % g->tz) continue;
         g->ncol = s->ncol > 0 ? s->ncol : elp_pick_ncol(g->tx);

@@ -59,6 +59,31 @@ def test_gpupol_cli_resume_is_bit_identical(tmp_path):
     assert "Executable = efpol" in s and "Npol = 393" in s
 
 
+@pytest.mark.parametrize("L", [64, 48])
+def test_tiled_run_names_its_clock(tmp_path, L):
+    """A tiled run writes Executable = elp_<tile shape>; the shape has a
+    measured time factor, and bin/elp_ne_list gives the analysis its line
+    (Ne of efpol, tFac / f) from efpol's."""
+    import elp
+    d = tmp_path / "run"
+    r = subprocess.run([os.path.join(BIN, "gpupol3_cuda_ring"), "100", "40", "7", str(d), "1.2", "0", "20", str(L),
+                        str(L), str(L)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    s = (d / "simulation_settings.txt").read_text()
+    exe = [ln.split(" = ")[1] for ln in s.splitlines() if ln.startswith("Executable = ")][0]
+    assert exe.startswith("elp_"), exe
+    tile = tuple(int(v) for v in exe[len("elp_"):].split("x"))
+    f = elp.time_factor(0, *tile)
+    assert 0 < f < 1
+    ne = tmp_path / "ne_list.dat"
+    ne.write_text("efpol 1.2 124 1.08 0.85 30\n")
+    lines = subprocess.run([os.path.join(BIN, "elp_ne_list"), str(ne)], capture_output=True, text=True,
+                           check=True).stdout.splitlines()
+    mine = [ln.split() for ln in lines if ln.startswith(exe + " ")]
+    assert len(mine) == 1 and mine[0][1] == "1.2" and mine[0][2] == "124"
+    assert abs(float(mine[0][4]) - 0.85 / f) < 1e-3
+
+
 def _ptl_from_tuv_files(d, times):
     """The per-ring files the reference's create_ptl would build from the TUV
     dumps in d (analysis/create_ptl.c:46-115), made by the writer the tests pin

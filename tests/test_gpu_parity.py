@@ -182,6 +182,21 @@ def test_large_box_invariants_and_conservation():
     assert counts == 5000 * 4027
 
 
+def test_default_tile_shapes():
+    """The default geometry follows the box: whole box up to L=32, then the
+    tile shape with the highest measured physical rate (attempted moves/s
+    times the shape's time factor): 16^3 below L=128, 32x16x16 from 128 to
+    256, 32^3 above.  Every default shape has a measured time factor."""
+    for L, N, tile in [(32, 100, None), (48, 100, (16, 16, 16)), (64, 200, (16, 16, 16)), (128, 1000, (32, 16, 16)),
+                       (256, 5000, (32, 16, 16)), (320, 5000, (32, 32, 32))]:
+        i = elp.Melt(L=L, N=N, seed=1).info()
+        if tile is None:
+            assert i.periodic == 1
+            continue
+        assert i.periodic == 0 and tuple(i.tile) == tile and i.specialised == 1, (L, tuple(i.tile))
+        assert elp.time_factor(0, *tile) > 0
+
+
 def test_l128_matches_replay():
     """The single large melt L=128, N=1000 (2517 rings), default geometry."""
     m = elp.Melt(L=128, N=1000, seed=7)

@@ -135,13 +135,14 @@ def test_small_jobs_pass_a_job_waiting_for_memory():
     memory frees up."""
     big = 2 * (64 ** 3 * 4 + 1573 * 16)
     srv = elp.Server(quantum=50, hbm_budget=int(1.5 * big))
-    first = srv.submit(2000, L=64, N=200, seed=41)            # resident
+    first = srv.submit(50000, L=64, N=200, seed=41)           # resident for about a second
     time.sleep(0.05)
     waiting = srv.submit(100, L=64, N=200, seed=42)           # does not fit beside it
     small = [srv.submit(100, L=16, N=50, seed=43 + i) for i in range(4)]
     srv.drain(300)
     res = {r["id"]: r for r in srv.poll()}
     assert all(r["status"] == 0 for r in res.values())
+    assert all(res[s]["t_start"] < res[first]["t_done"] for s in small), "the resident job ended too early"
     assert all(res[s]["t_start"] < res[waiting]["t_start"] for s in small)
     assert res[waiting]["t_start"] >= res[first]["t_done"] - 0.05
     srv.close()

@@ -83,16 +83,18 @@ def test_statistics_match_reference_efpol(name, seeds, linear):
         assert d <= Z * se, f"{key}[{idx}]: efpol {ma:.5g} vs GPU {mg:.5g} differ by {d:.3g} > {Z} x {se:.3g}"
 
 
-# Tiled geometries: L=64 melts run as 32^3 tiles (the default at L=64 and
-# L=256) or 32x16x16 tiles (the default at L=128).  A move whose footprint
-# crosses a tile wall is rejected, as gpupol's out-of-block moves are
-# (gpupol2/ringpol3.cu:58-76); the walls move every step, so the equilibrium
-# (Rg^2, stored length, run lengths) is efpol's, compared here over steps
-# 15000-50000, while the clock runs slower: the GPU's centre-of-mass MSD
-# after t steps is efpol's after f*t steps, f the time factor that
-# elp_time_factor records for the shape (and the drop-in programs hand to
-# the analysis through their Executable name).
-TILED = [((32, 32, 32), range(7001, 7009)), ((32, 16, 16), range(7101, 7109))]
+# Tiled geometries: L=64 melts run as 32^3 tiles (the default at L > 256
+# and the largest specialised shape), 32x16x16 tiles (the default at
+# L = 128 and 256) or 16x16x8 tiles (the smallest shape of the default list,
+# on the generic kernel).  A move whose footprint crosses a tile wall is
+# rejected, as gpupol's out-of-block moves are (gpupol2/ringpol3.cu:58-76);
+# the walls move every step, so the equilibrium (Rg^2, stored length, run
+# lengths) is efpol's, compared here over steps 15000-50000, while the clock
+# runs slower: the GPU's centre-of-mass MSD after t steps is efpol's after
+# f*t steps, f the time factor that elp_time_factor records for the shape
+# (and the drop-in programs hand to the analysis through their Executable
+# name).
+TILED = [((32, 32, 32), range(7001, 7009)), ((32, 16, 16), range(7101, 7109)), ((16, 16, 8), range(7801, 7809))]
 
 
 def msd_step_ratio(lags, ref_msd, msd):
