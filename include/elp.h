@@ -313,8 +313,11 @@ void elp_batch_destroy(elp_batch* b);
  * on chip and every tile shape that divides the box, each with 1, 10 or 100
  * steps per launch -- on `copies` copies of its initial melt run as one batch
  * for `steps` steps, and returns the fastest as an explicit spec (periodic,
- * tile, ncol, steps_per_launch filled in).  Whole-box domains have no tile
- * walls, so a tiled shape is chosen only when it is over 1.5x faster.  The tile shape is part of a
+ * tile, ncol, steps_per_launch filled in).  "Fastest" is the time per
+ * efpol-equivalent step: the time per step divided by the geometry's clock
+ * factor (elp_time_factor; 1 for the wall-free whole box), so tile walls
+ * cost what they slow the melt; shapes without a measured factor are not
+ * candidates.  The tile shape is part of a
  * trajectory's definition: record the returned spec and reuse it; runs of the
  * same spec give the same bits, alone or batched. */
 elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32_t steps, elp_job_spec* out,

@@ -15,6 +15,7 @@
 #include <map>
 #include <new>
 #include <tuple>
+#include <algorithm>
 #include <vector>
 
 #include "elp_common.h"
@@ -381,6 +382,13 @@ extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info
 }
 
 // ---- autotuner ---------------------------------------------------------------
+// Clock factor of a candidate: 1 for the whole box, the measured time factor
+// of its tile shape, 0 if that shape was not measured.
+static double clock_factor(const elp_job_spec& c)
+{
+    return c.periodic == 1 ? 1.0 : elp_time_factor(0, c.tile[0], c.tile[1], c.tile[2]);
+}
+
 // Candidate geometries for a melt: its whole box on chip (if that fits) and
 // every tile shape of the preference list that divides the box, each with a
 // few steps-per-launch values.  Each is timed on `copies` copies of the initial melt
@@ -424,6 +432,9 @@ extern "C" elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32
             cand.push_back(s);
         }
     }
+    // a shape whose clock was never measured cannot be compared
+    cand.erase(std::remove_if(cand.begin(), cand.end(), [](const elp_job_spec& c) { return clock_factor(c) <= 0.0; }),
+               cand.end());
     if (cand.empty()) return elp_fail(ELP_ERR_ARG, "no candidate geometry for L=%d", in->L);
     float best = -1.f, best_score = 0.f;
     for (const elp_job_spec& c : cand) {
@@ -437,10 +448,11 @@ extern "C" elp_status elp_autotune(const elp_job_spec* in, int32_t copies, int32
         if (st == ELP_OK) st = elp_batch_run_timed(b, steps, &ms);
         elp_batch_destroy(b);
         if (st != ELP_OK) continue;
-        // Whole-box domains have no tile walls (no rejected boundary moves), so
-        // a tiled shape must be clearly faster to be preferred.
+        // Tile walls slow the melt's clock: a tiled step moves the rings as
+        // far as f efpol steps (f measured per shape, 1 for the wall-free
+        // whole box), so candidates compete on time per efpol-equivalent step.
         const float per = ms / (float)steps;
-        const float score = c.periodic == 1 ? per / 1.5f : per;
+        const float score = per / (float)clock_factor(c);
         if (best < 0.f || score < best_score) {
             best = per;
             best_score = score;

@@ -80,3 +80,23 @@ def test_several_tiles_per_cta_give_the_same_bits():
         wb, rb = m.state()
         assert np.array_equal(wa, wb) and np.array_equal(ra, rb), f"member {j} differs from its single run"
         assert b.check(j) == 0
+
+
+@pytest.mark.parametrize("L,N", [(32, 100), (64, 200)])
+def test_autotune_returns_a_geometry_with_a_known_clock(L, N):
+    """The autotuner ranks candidates by time per efpol-equivalent step, so
+    its choice always has a measured clock factor, and the returned spec
+    runs and gives the same bits alone and batched."""
+    sp, ms = elp.autotune(copies=4, steps=10, L=L, N=N, seed=9)
+    assert ms > 0
+    f = 1.0 if sp["periodic"] == 1 else elp.time_factor(0, *sp["tile"])
+    assert 0 < f <= 1
+    m = elp.Melt(**sp)
+    m.init_melt()
+    m.run(10)
+    b = elp.Batch([sp, dict(sp, seed=10)])
+    b.init_melts()
+    b.run(10)
+    w, r = m.state()
+    wb, rb = b.state(0)
+    assert np.array_equal(w, wb) and np.array_equal(r, rb)
