@@ -140,7 +140,7 @@ elp_status elp_device_errors(const uint32_t* d_flags, cudaStream_t s)
 void elp_walk_bufs_free(elp_walk_bufs* b)
 {
     cudaFree(b->d_start); cudaFree(b->d_bonds); cudaFree(b->d_status); cudaFree(b->d_visit); cudaFree(b->d_cnt);
-    cudaFree(b->d_obs);
+    cudaFree(b->d_obs); cudaFree(b->d_rank); cudaFree(b->d_total);
     cudaFreeHost(b->h_status); cudaFreeHost(b->h_cnt);
     *b = elp_walk_bufs();
 }
@@ -178,11 +178,18 @@ elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int 
 {
     elp_status st = elp_walk_bufs_reserve(b, P, N, 0);
     if (st) return st;
-    WalkArgs w;
-    memset(&w, 0, sizeof(w));
-    w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P; w.linear = linear;
-    w.start = b->d_start; w.bonds = b->d_bonds; w.status = b->d_status;
-    ELP_CUDA_TRY(elp_launch_walk(&w, s));
+    // list ranking: every run at once, ceil(log2 N) rounds; the chain walk
+    // (one ring's latency) for boxes too large for its scratch
+    const cudaError_t re = elp_rank_chains(lat, rec, L, N, P, linear, b, s);
+    if (re == cudaErrorNotSupported) {
+        WalkArgs w;
+        memset(&w, 0, sizeof(w));
+        w.lat = lat; w.rec = rec; w.L = L; w.N = N; w.P = P; w.linear = linear;
+        w.start = b->d_start; w.bonds = b->d_bonds; w.status = b->d_status;
+        ELP_CUDA_TRY(elp_launch_walk(&w, s));
+    } else {
+        ELP_CUDA_TRY(re);
+    }
     std::vector<int32_t> status((size_t)P);
     ELP_CUDA_TRY(cudaMemcpyAsync(start, b->d_start, (size_t)P * 3 * 4, cudaMemcpyDeviceToHost, s));
     ELP_CUDA_TRY(cudaMemcpyAsync(bonds, b->d_bonds, (size_t)P * N, cudaMemcpyDeviceToHost, s));

@@ -36,7 +36,9 @@ struct elp_walk_bufs {
     unsigned long long* d_obs = nullptr;   // observables: [P][6] ring sums + histogram
     int32_t* h_status = nullptr;           // pinned host copies of the ring statuses and counters
     unsigned long long* h_cnt = nullptr;
-    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0, cap_obs = 0, cap_h_rings = 0;
+    void* d_rank = nullptr;                // list ranking: 20 bytes a site (elp_rank.cu)
+    uint32_t* d_total = nullptr;           // list ranking: monomers per chain
+    size_t cap_rings = 0, cap_bonds = 0, cap_sites = 0, cap_obs = 0, cap_h_rings = 0, cap_rank_sites = 0, cap_total = 0;
     size_t bytes = 0;
 };
 void elp_walk_bufs_free(elp_walk_bufs* b);
@@ -51,6 +53,14 @@ elp_status elp_build_melt(uint32_t* lat, uint32_t* rec, int L, int N, int P, int
 // stream-ordered: no transfer, no host wait.
 elp_status elp_init_melt_device(uint32_t* lat, uint32_t* rec, int L, int N, int P, int linear, cudaStream_t s);
 
+// Boxes up to this many sites (L = 512) rebuild their chains by list
+// ranking; larger ones by the chain walk.
+constexpr size_t ELP_RANK_MAX_SITES = (size_t)1 << 27;
+// Chains of one melt into b->d_start / d_bonds / d_status by list ranking
+// (elp_rank.cu), stream-ordered; cudaErrorNotSupported (nothing launched)
+// above ELP_RANK_MAX_SITES sites.
+cudaError_t elp_rank_chains(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear,
+                            elp_walk_bufs* b, cudaStream_t s);
 // Rebuild rings (start[3P], bonds[P*N]) of one melt into host buffers.
 elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                            int32_t* start, uint8_t* bonds, cudaStream_t s);
