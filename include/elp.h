@@ -73,6 +73,8 @@ typedef struct elp_info {
     uint64_t step;            /* absolute steps done */
     uint64_t device_bytes;    /* device memory held by the context */
     int32_t linear;           /* 1: linear chains */
+    uint64_t kernels;         /* kernels launched for the sweep so far (a CUDA-graph replay counts its
+                                 kernels: its sweep launches and the step-counter update) */
 } elp_info;
 
 /* Fill a spec with defaults: density 1.2, auto geometry, device 0. */

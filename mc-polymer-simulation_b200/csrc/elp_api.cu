@@ -318,6 +318,7 @@ extern "C" elp_status elp_get_info(const elp_ctx* c, elp_info* info)
     info->step = elp_group_step(&c->G, 0);
     info->device_bytes = c->device_bytes + c->wb.bytes;
     info->linear = c->linear;
+    info->kernels = c->G.kernels;
     return ELP_OK;
 }
 

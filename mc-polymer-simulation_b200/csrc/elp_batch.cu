@@ -378,6 +378,7 @@ extern "C" elp_status elp_batch_job_info(const elp_batch* b, int32_t j, elp_info
     info->smem_bytes = G->smem;
     info->step = elp_group_step(G, mm.index);
     info->device_bytes = b->device_bytes + b->wb.bytes;
+    info->kernels = G->kernels;   // of the member's geometry group
     return ELP_OK;
 }
 

@@ -173,11 +173,24 @@ elp_status elp_walk_bufs_reserve(elp_walk_bufs* b, int P, int N, size_t sites)
     return ELP_OK;
 }
 
+// Pinned host copy of the chain statuses (the copy runs behind the kernels).
+static elp_status reserve_host_status(elp_walk_bufs* b, int P)
+{
+    if ((size_t)P > b->cap_h_rings) {
+        cudaFreeHost(b->h_status);
+        b->h_status = nullptr;
+        b->cap_h_rings = 0;
+        ELP_CUDA_TRY(cudaMallocHost((void**)&b->h_status, (size_t)P * sizeof(int32_t)));
+        b->cap_h_rings = (size_t)P;
+    }
+    return ELP_OK;
+}
+
 elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int N, int P, int linear, elp_walk_bufs* b,
                            int32_t* start, uint8_t* bonds, cudaStream_t s)
 {
     elp_status st = elp_walk_bufs_reserve(b, P, N, 0);
-    if (st) return st;
+    if (st || (st = reserve_host_status(b, P))) return st;
     // list ranking: every run at once, ceil(log2 N) rounds; the chain walk
     // (one ring's latency) for boxes too large for its scratch
     const cudaError_t re = elp_rank_chains(lat, rec, L, N, P, linear, b, s);
@@ -190,14 +203,13 @@ elp_status elp_fetch_rings(const uint32_t* lat, const uint32_t* rec, int L, int 
     } else {
         ELP_CUDA_TRY(re);
     }
-    std::vector<int32_t> status((size_t)P);
     ELP_CUDA_TRY(cudaMemcpyAsync(start, b->d_start, (size_t)P * 3 * 4, cudaMemcpyDeviceToHost, s));
     ELP_CUDA_TRY(cudaMemcpyAsync(bonds, b->d_bonds, (size_t)P * N, cudaMemcpyDeviceToHost, s));
-    ELP_CUDA_TRY(cudaMemcpyAsync(status.data(), b->d_status, (size_t)P * 4, cudaMemcpyDeviceToHost, s));
+    ELP_CUDA_TRY(cudaMemcpyAsync(b->h_status, b->d_status, (size_t)P * 4, cudaMemcpyDeviceToHost, s));
     ELP_CUDA_TRY(cudaStreamSynchronize(s));
     for (int p = 0; p < P; p++)
-        if (status[(size_t)p])
-            return elp_fail(ELP_ERR_INTEGRITY, "ring %d cannot be walked (code %d)", p, status[(size_t)p]);
+        if (b->h_status[p])
+            return elp_fail(ELP_ERR_INTEGRITY, "chain %d is broken (code %d)", p, b->h_status[p]);
     return ELP_OK;
 }
 
@@ -207,13 +219,7 @@ elp_status elp_fetch_checked_melt(const uint32_t* lat, const uint32_t* rec, int 
     const size_t S = (size_t)L * L * L;
     elp_status st = elp_walk_bufs_reserve(b, P, N, S);
     if (st) return st;
-    if ((size_t)P > b->cap_h_rings) {
-        cudaFreeHost(b->h_status);
-        b->h_status = nullptr;
-        b->cap_h_rings = 0;
-        ELP_CUDA_TRY(cudaMallocHost((void**)&b->h_status, (size_t)P * sizeof(int32_t)));
-        b->cap_h_rings = (size_t)P;
-    }
+    if ((st = reserve_host_status(b, P))) return st;
     if (!b->h_cnt) ELP_CUDA_TRY(cudaMallocHost((void**)&b->h_cnt, 8 * sizeof(unsigned long long)));
     ELP_CUDA_TRY(cudaMemsetAsync(b->d_visit, 0, S * sizeof(uint32_t), s));
     ELP_CUDA_TRY(cudaMemsetAsync(b->d_cnt, 0, 8 * sizeof(unsigned long long), s));

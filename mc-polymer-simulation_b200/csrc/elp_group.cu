@@ -67,6 +67,7 @@ cudaError_t launch_generic(elp_group* G, int nsteps)
         int threads = (G->lay.groups + 31) / 32 * 32;
         cudaError_t e = elp_launch_sweep(&a, domains_of(G->g), threads < 32 ? 32 : threads, G->lay.bytes, G->stream);
         if (e != cudaSuccess) return e;
+        G->kernels++;
     }
     return cudaSuccess;
 }
@@ -75,6 +76,7 @@ cudaError_t launch_once(elp_group* G, int nsteps, uint32_t step_base)
 {
     if (!G->specialised) return launch_generic(G, nsteps);
     Sweep2Launch l = make_launch(G, nsteps, step_base, 0);
+    G->kernels++;
     return elp_launch_sweep2(&l, G->stream);
 }
 }  // namespace
@@ -217,6 +219,7 @@ cudaError_t elp_group_run(elp_group* G, int64_t nsteps)
         }
         while (nsteps >= gsteps) {
             if ((e = cudaGraphLaunch(G->graph, G->stream)) != cudaSuccess) return e;
+            G->kernels += (uint64_t)(gsteps / k + 1);   // its sweep launches and the counter update
             G->steps_done += (uint64_t)gsteps;
             G->ctr_mirror += (uint32_t)gsteps;
             nsteps -= gsteps;

@@ -39,6 +39,7 @@ struct elp_group {
     int hold_cta1 = 0;                // test hook: CTA + 1 that never arrives at the first barrier
     uint64_t steps_done = 0;          // steps since the job table's step0 values
     uint32_t ctr_mirror = 0;          // host copy of *d_ctr
+    uint64_t kernels = 0;             // sweep-path kernels launched (graph replays count their nodes)
 
     cudaGraphExec_t graph = nullptr;
     uint32_t graph_base = 0;          // step_base offset the graph was captured with

@@ -35,7 +35,7 @@ class Info(C.Structure):
     _fields_ = [("L", C.c_int32), ("N", C.c_int32), ("P", C.c_int32), ("periodic", C.c_int32),
                 ("tile", C.c_int32 * 3), ("ncol", C.c_int32), ("domains", C.c_int32), ("threads", C.c_int32),
                 ("specialised", C.c_int32), ("smem_bytes", C.c_uint64), ("step", C.c_uint64), ("device_bytes", C.c_uint64),
-                ("linear", C.c_int32)]
+                ("linear", C.c_int32), ("kernels", C.c_uint64)]
 
 
 EXPORTED = [

@@ -91,3 +91,22 @@ def test_limits_refused_cleanly(tmp_path):
     with pytest.raises(elp.ElpError) as e:
         m.load_tuv(str(p))
     assert e.value.status == elp.ERR_FORMAT
+
+
+def test_kernel_count_of_a_run():
+    """elp_info.kernels counts the sweep path's kernels: one per launch, and
+    a CUDA-graph replay (tiled melts, 100 steps per graph) its launches plus
+    the step-counter update."""
+    m = elp.Melt(L=16, N=50, seed=3, steps_per_launch=10)     # whole box: direct launches
+    m.init_melt()
+    k0 = m.info().kernels
+    m.run(35)
+    assert m.info().kernels - k0 == 4
+    m = elp.Melt(L=64, N=200, seed=3, periodic=0, tile=(32, 32, 32), steps_per_launch=20)
+    m.init_melt()
+    k0 = m.info().kernels
+    m.run(20)                      # fewer steps than a graph: one launch
+    assert m.info().kernels - k0 == 1
+    m.run(230)                     # two graph replays of 5 launches + counter, then 30 steps: 2 launches
+    assert m.info().kernels - k0 == 1 + 2 * 6 + 2
+    assert m.check() == 0

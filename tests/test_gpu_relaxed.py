@@ -181,7 +181,7 @@ def test_crowded_tiles_take_the_general_move(L, N, kw, spl):
 
 
 @pytest.mark.parametrize("L,N,seed,spl,relax,steps,every", [
-    (128, 1000, 7, 20, 2000, 50, 10),     # the bench's headline melt, its geometry and launch shape
+    (128, 1000, 7, 100, 2000, 50, 10),    # the bench's headline melt, its geometry and launch shape
     (256, 5000, 11, 10, 2000, 10, 5),     # the roofline melt
 ])
 def test_bench_melts_relaxed_match_replay(L, N, seed, spl, relax, steps, every):
