@@ -114,7 +114,8 @@ struct Shape {
     static constexpr int OFFW = TABW + 1024;
     static constexpr int WOFFW = OFFW + NOFF;
     static constexpr int COLW = WOFFW + (PER ? 0 : 16);
-    static constexpr int SCHW = COLW + 64;
+    static constexpr int SHFW = COLW + 64;    // the step's domain shift (tiles), drawn by one warp
+    static constexpr int SCHW = SHFW + 4;
     static constexpr int SSOW = SCHW + CAP;   // {offset of monomer 0 in its run (bits 0-15), site word (16-31)}
     static constexpr int NSLW = SSOW + CAP;
     static constexpr int HTABW = NSLW + 1;    // table rows (0xf, x): moves of a linear chain's monomer 0
@@ -381,6 +382,7 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
     uint8_t* tab = reinterpret_cast<uint8_t*>(g_smem + TABW);
     int* offs = reinterpret_cast<int*>(g_smem + OFFW);
     uint32_t* col = g_smem + SH::COLW;
+    uint32_t* shf = g_smem + SH::SHFW;
     uint32_t* slot_chain = g_smem + SH::SCHW;
     uint32_t* slot_so = g_smem + SH::SSOW;
     uint32_t* nslots = g_smem + SH::NSLW;
@@ -485,14 +487,22 @@ __global__ void __launch_bounds__(THREADS, MINB) sweep2_kernel(BatchLaunch a)
 
         for (int st = 0; st < inner && !overflow; st++) {
             const uint32_t t = J.step0 + a.step_base + step_dev + (uint32_t)(so + st);
-            if (!PER) {
+            if (!PER && tid < 32) {
+                // one warp draws the step's domain shift for the whole CTA
                 const uint4 sh = philox(make_uint4(t, 0, ELP_STREAM_SHIFT, 0), key);
-                D.x0 = (int)bounded(sh.x, TX) + (d % ntx) * TX;
-                D.y0 = (int)bounded(sh.y, TY) + ((d / ntx) % nty) * TY;
-                D.z0 = (int)bounded(sh.z, TZ) + (d / ntx / nty) * TZ;
+                if (tid == 0) {
+                    shf[0] = bounded(sh.x, TX);
+                    shf[1] = bounded(sh.y, TY);
+                    shf[2] = bounded(sh.z, TZ);
+                }
             }
             if (st == 0) {
-                __syncthreads();  // the previous item's stores have read shared memory
+                __syncthreads();  // the previous item's stores have read shared memory; the shift is written
+                if (!PER) {
+                    D.x0 = (int)shf[0] + (d % ntx) * TX;
+                    D.y0 = (int)shf[1] + ((d / ntx) % nty) * TY;
+                    D.z0 = (int)shf[2] + (d / ntx / nty) * TZ;
+                }
                 if (tid == 0) *nslots = 0;
                 const bool few = nchains <= THREADS;  // few rings: find monomer 0 through the records
                 if (PER) {
