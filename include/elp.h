@@ -116,11 +116,16 @@ void* elp_stream(elp_ctx* ctx);
 elp_status elp_sync(elp_ctx* ctx);
 
 /* Rebuild the rings on the device and copy them to host buffers
- * start[3*P] (int32) and bonds[P*N] (uint8).  Blocking.  Returns
- * ELP_ERR_STATE if an earlier launch reported an error (as elp_sync), else
- * ELP_ERR_INTEGRITY if a ring cannot be walked; on either error the
- * buffers' contents are unspecified.  With pinned buffers the copies run
- * asynchronously behind the walk, itself queued behind the steps. */
+ * start[3*P] (int32) and bonds[P*N] (uint8).  Blocking.  The rings are
+ * rebuilt by list ranking over all runs at once (boxes up to L = 512; a
+ * walk along each ring above).  Returns ELP_ERR_STATE if an earlier launch
+ * reported an error (as elp_sync), else ELP_ERR_INTEGRITY if a chain is
+ * broken (a bond that is no lattice bond, a run leading to an empty site or
+ * into another chain, a wrong monomer count); on either error the buffers'
+ * contents are unspecified.  With pinned buffers the copies run
+ * asynchronously behind the kernels, themselves queued behind the steps.
+ * Replaces GPULatticeToCPU + the host's ring rebuild
+ * (gpupol2/gpupol_cuda.cu:60, gpupol2/oclpol.c:183-376). */
 elp_status elp_fetch_chains(elp_ctx* ctx, int32_t* start, uint8_t* bonds);
 
 /* elp_fetch_chains and elp_check in one pass over the melt (one ring walk,
